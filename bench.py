@@ -1,0 +1,315 @@
+"""Benchmark: photons/s of the MCML photon walk on one B200 (or N replicas, one per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload skin5|slab_n14] [--impl b200|reference]
+
+A step is one full run of the workload: 'skin5' (default; five-layer skin stack, 1e8 photons,
+nr=500 x nz=400 A(r,z), 30 exit-angle bins) or 'slab_n14' (one slab, 1e6 photons). `value` times
+the walk kernel (with its tally zeroing) on the device with CUDA events on the launching stream,
+L2 flushed between steps; `e2e` times the public C-ABI call tmc_b200_run with host buffers (the
+run description goes in through the kernel parameters, the fixed-point tallies come back to host
+memory and are decoded) by the host clock. `cpu_baseline` and `--impl reference` time the
+reference's own multithreaded CPU engine (oracle/_ref/tissuemc, built from TissueMC's sources) on
+a bounded sample of the same workload on this host's cores.
+
+Under torchrun (N > 1) every rank runs its own replica of the workload (independent seeds): the
+walk has no exchange step, so there is no collective in the data path; ranks meet only at the
+barriers around the timed region, and the slowest rank's time is reported.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "skin5": "five-layer skin stack (n=1.4 in air; 1e8 photons; dr=0.002 cm x 500, dz=0.001 cm x 400, na=30)",
+    "slab_n14": "single slab n=1.4 in air (mua=5, mus=95, g=0.8, d=0.05 cm; 1e6 photons; 50x20 grid, na=30)",
+}
+METRIC = "photons/s on 1 B200 (plain MC)"
+
+# Algorithmic work of the walk, counted from the reference's step (include/tissuemc/physics.hpp
+# :148-193 and :101-144 with the scoring) and frozen here: FP32 operations and SFU operations
+# (log, sqrt, rsqrt, sin, cos, reciprocal of a division) per interaction step and per boundary
+# step. The issue roofline of one SM is 128 FP32 lanes and 16 SFU lanes per clock.
+F_INT, S_INT = 61, 12
+F_BND, S_BND = 25, 3
+# Interaction and boundary steps per photon, measured with the float64 oracle (seed 1).
+STEPS_PER_PHOTON = {"skin5": (604.20, 14.30), "slab_n14": (19.71, 2.03)}
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="skin5", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--batches", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--photons", type=int, default=0,
+                    help="override the workload's photon count (for profiling captures only)")
+    return ap.parse_args()
+
+
+def _dist():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def _peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (SM clock and throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9], strict=False):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _cpu_info() -> tuple[str, int]:
+    model = "unknown"
+    try:
+        m = re.search(r"model name\s*:\s*(.+)", Path("/proc/cpuinfo").read_text())
+        model = m.group(1).strip() if m else model
+    except OSError:
+        pass
+    return model, os.cpu_count() or 1
+
+
+def reference_cpu_sample(workload: str, target_s: float = 12.0) -> dict:
+    """Time the reference's own CPU engine (all host threads) on a bounded sample of the workload:
+    a short pilot sizes the sample to about `target_s` seconds."""
+    import oracle
+
+    if not oracle.reference_available():
+        raise RuntimeError("oracle/_ref/tissuemc is missing (built by `make -C oracle` where the reference sources are)")
+    text = (ROOT / "tissuemc_b200" / "configs" / f"{workload}.mci").read_text()
+    model, cores = _cpu_info()
+    batches = max(10, 4 * cores)
+    pilot = 20 * batches if workload == "skin5" else 2000 * batches
+    r = oracle.run_reference(text, pilot, batches, 1, "float64", threads=0)
+    rate = r["photons"] / max(r["wall_seconds"], 1e-3)
+    n = max(batches, int(rate * target_s) // batches * batches)
+    r = oracle.run_reference(text, n, batches, 1, "float64", threads=0)
+    return {"value": r["photons"] / r["wall_seconds"], "unit": "photons/s", "cores": r["threads"],
+            "kind": "reference", "seconds": r["wall_seconds"],
+            "sample": f"{n} photons of {workload} ({batches} batches, float64, reference CPU engine "
+                      f"oracle/_ref/tissuemc, {r['threads']} threads on {model})"}
+
+
+def run_reference_arm(a) -> None:
+    rank, world, _ = _dist()
+    if rank != 0:
+        return
+    vals, secs = [], []
+    for _ in range(a.warmup):
+        reference_cpu_sample(a.workload, target_s=3.0)
+    for _ in range(a.steps):
+        s = reference_cpu_sample(a.workload, target_s=8.0)
+        vals.append(s["value"])
+        secs.append(s["seconds"])
+    v = sum(vals) / len(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "photons/s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the workload's .mci; seeded Philox photons)",
+            "config": {"workload": f"{a.workload}: {WORKLOADS[a.workload]}", "photons_per_step": "bounded sample"},
+            "cpu_baseline": {k: s[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": "photons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["cpu_baseline"]["value"] = v
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    a = _args()
+    if a.impl == "reference":
+        run_reference_arm(a)
+        return
+    import ctypes
+
+    import torch
+
+    import tissuemc_b200 as tmc
+
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    spec = tmc.workload(a.workload)
+    if a.photons:
+        spec.photons = a.photons
+    photons = spec.photons
+    opt = tmc.options(batches=a.batches, seed=1 + 1000003 * rank, device=local)
+    words = int(tmc.query_sizes(spec, opt).tally_words)
+    d_tally = torch.empty(words, dtype=torch.int64, device=f"cuda:{local}")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    stream = torch.cuda.Stream(device=local)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    def step() -> float:
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)  # evict L2 between steps (outside the timed events)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            tmc.run_device(spec, opt, d_tally.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(a.warmup):
+        step()
+    barrier()
+    with Clocks(local) as clk:
+        times = [step() for _ in range(a.steps)]
+        barrier()
+    total_ms = sum(times)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms = total_ms / a.steps
+    value = world * photons / (ms / 1e3)
+
+    # end to end through the public C ABI with host buffers
+    e2e_times = []
+    sz = tmc.query_sizes(spec, opt)
+    for i in range(a.steps + 1):
+        t0 = time.perf_counter()
+        res = tmc.run(spec, opt)
+        if i:  # the first call is a warm-up
+            e2e_times.append(time.perf_counter() - t0)
+    e2e_s = sum(e2e_times) / len(e2e_times)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * photons / e2e_s, "unit": "photons/s",
+           "h2d_bytes_per_step": int(ctypes.sizeof(tmc.CRunSpec) + ctypes.sizeof(tmc.COptions)),
+           "d2h_bytes_per_step": int(sz.tally_words) * 8}
+
+    if rank == 0:
+        peaks = _peaks()
+        f_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+        n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+        e_int, e_bnd = STEPS_PER_PHOTON[a.workload]
+        f_tot = e_int * F_INT + e_bnd * F_BND
+        s_tot = e_int * S_INT + e_bnd * S_BND
+        clocks_per_photon = max(f_tot / 128.0, s_tot / 16.0) / n_sm  # SM-clocks per photon, whole GPU
+        peak = f_mhz * 1e6 / clocks_per_photon
+        achieved = photons / (ms / 1e3)
+        line = {
+            "metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 transport, u64 fixed-point tallies",
+            "data": "synthetic (the workload's .mci; seeded Philox photons)",
+            "config": {"workload": f"{a.workload}: {WORKLOADS[a.workload]}", "photons_per_step": photons,
+                       "batches": a.batches, "l2": "flushed between steps (256 MB write)",
+                       "parallelism": "replicas" if world > 1 else "1 GPU"},
+            "e2e": e2e,
+            "gpu_launches": a.steps,
+            "roofline": {
+                "bound": "sfu" if s_tot / 16.0 >= f_tot / 128.0 else "fp32", "achieved": achieved / 1e9,
+                "peak": peak / 1e9, "unit": "Gphotons/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": f"issue roofline: {n_sm} SMs x {f_mhz:.0f} MHz (sm_max_mhz of MEASURED_PEAKS.json) / "
+                               f"max(F/128, S/16) with F={f_tot:.0f} FP32 and S={s_tot:.0f} SFU ops per photon",
+            },
+            "clocks": clk.summary(),
+            "kernel_ms_per_step": ms,
+            "device": res.device,
+        }  # fmt: skip
+        if not a.no_cpu_baseline and world == 1:
+            try:
+                line["cpu_baseline"] = reference_cpu_sample(a.workload)
+                line["cpu_baseline"].pop("seconds", None)
+            except Exception as exc:  # report, never fake
+                line["cpu_baseline"] = {"unavailable": str(exc)}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

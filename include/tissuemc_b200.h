@@ -1,0 +1,186 @@
+/* tissuemc_b200.h — C ABI of the B200 (sm_100a) photon-walk engine.
+ *
+ * The engine is a drop-in for TissueMC's GPU engine, whose C++ boundary is
+ *
+ *     namespace tissuemc {
+ *         bool cuda_available();                                            // cuda_engine.hpp:9-11
+ *         RunResult run_cuda(const RunSpec &run, const EngineOptions &opt); // cuda_engine.hpp:13-14
+ *     }
+ *
+ * (paths relative to the TissueMC project root: include/tissuemc/cuda_engine.hpp). The entry points
+ * below carry the same information as plain C structs, pointers and sizes, so that the C++ shim
+ * (tissuemc_b200/csrc/host/run_cuda.cpp), ctypes, or any other FFI can bind them. Results are
+ * written into caller-allocated buffers whose sizes come from tmc_b200_query_sizes().
+ *
+ * Every entry point is synchronous at the boundary, uses the device given in the options (default
+ * 0) and is NOT re-entrant: concurrent calls from several host threads must be serialised by the
+ * caller, as with the reference engine (src/cuda/engine.cu:322-358 runs on the default stream of
+ * device 0).
+ *
+ * Status codes follow the reference's error behaviour: an invalid run or invalid options is
+ * TMC_BAD_CONFIG (the reference throws ConfigError, config.hpp:31-66 and engine.cu:328-350), a
+ * missing device is TMC_NO_DEVICE ("no usable CUDA device found", engine.cu:351-353), a CUDA
+ * failure is TMC_CUDA_ERROR ("CUDA error at file:line: ...", engine.cu:18-26). The message buffer
+ * holds the same text the reference would put in the exception.
+ */
+#ifndef TISSUEMC_B200_H
+#define TISSUEMC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The library exports these entry points and nothing else (its C++ internals are hidden). */
+#if defined(__GNUC__)
+#define TMC_B200_API __attribute__((visibility("default")))
+#else
+#define TMC_B200_API
+#endif
+
+#define TMC_B200_MAX_LAYERS 16
+#define TMC_B200_ABI_VERSION 1
+
+typedef enum {
+    TMC_OK = 0,
+    TMC_BAD_CONFIG = 1,     /* invalid run description or options                           */
+    TMC_NO_DEVICE = 2,      /* no usable CUDA device                                         */
+    TMC_CUDA_ERROR = 3,     /* a CUDA runtime call failed                                    */
+    TMC_DEVICE_TIMEOUT = 4, /* a bounded device-side wait gave up (sweep work queue)         */
+    TMC_BAD_ARGUMENT = 5    /* a NULL pointer or a buffer too small for the run              */
+} tmc_status_code;
+
+typedef struct {
+    int32_t code;       /* tmc_status_code */
+    char message[512];  /* NUL-terminated; empty on success */
+} tmc_status;
+
+/* One tissue layer: refractive index, absorption and scattering coefficients [1/cm], anisotropy,
+ * thickness [cm]. Mirrors LayerSpec (include/tissuemc/config.hpp:14-20). */
+typedef struct {
+    double n, mua, mus, g, d;
+} tmc_layer;
+
+/* One MCML run. Mirrors RunSpec (include/tissuemc/config.hpp:22-29); na, which the reference
+ * parses but never uses, sets the number of exit-angle bins of R_d(r,a) and T_t(r,a). */
+typedef struct {
+    uint64_t photons;
+    double dz, dr;
+    int32_t nz, nr, na;
+    double n_above, n_below;
+    int32_t num_layers;
+    tmc_layer layers[TMC_B200_MAX_LAYERS];
+} tmc_run_spec;
+
+/* Engine options. Mirrors EngineOptions (include/tissuemc/cpu_engine.hpp:18-30) where the fields
+ * mean something to a GPU engine; zero-initialise and set what you need (tmc_b200_default_options
+ * fills the reference's defaults). */
+typedef struct {
+    uint64_t seed;          /* Philox key; photon i always uses the stream (seed, i)           */
+    int32_t batches;        /* >= 1 and <= photons; the unit of the standard error              */
+    uint64_t photons;       /* if nonzero, overrides spec.photons                               */
+    int32_t rung;           /* accepted for CLI compatibility: 0,1,3,5,6,7,8; one B200 kernel   */
+    int32_t profiles;       /* 0: skip the profile tallies (diagnostic, rung 6 only)            */
+    int32_t device;         /* CUDA device ordinal                                              */
+    int32_t fast_math;      /* 1 (default): SFU intrinsics; 0: IEEE division/sqrt, libdevice    */
+    int32_t threads_per_block; /* 0 = chosen by the planner                                     */
+    int32_t blocks_per_sm;     /* 0 = chosen by the planner                                     */
+    int32_t smem_budget;       /* bytes of shared memory per block for tallies; 0 = planner     */
+} tmc_options;
+
+/* Element counts of every output buffer for a run (tmc_b200_query_sizes). */
+typedef struct {
+    uint64_t batches, layers, nz, nr, na;
+    uint64_t absorbed; /* batches * layers */
+    uint64_t a_rz;     /* nr * nz  */
+    uint64_t ra;       /* nr * na  (each of rd_ra and tt_ra) */
+    uint64_t tally_words; /* 64-bit words of the raw fixed-point tally buffer */
+} tmc_sizes;
+
+/* Caller-allocated host buffers for one run. Every pointer is required unless marked optional.
+ * Weights are in units of launched packets (the sums the reference reports, not normalised per
+ * area or solid angle). 2-D arrays are row-major with r as the slow index, as MCML's A_rz[ir][iz]
+ * and Rd_ra[ir][ia]. */
+typedef struct {
+    uint64_t *first_photon, *photons; /* [batches]  BatchPlan (include/tissuemc/batching.hpp)   */
+    double *rd, *tt;                  /* [batches]  weight leaving through the top / bottom     */
+    double *absorbed;                 /* [batches * layers]                                      */
+    uint64_t *events, *anomalies;     /* [batches]                                               */
+    double *a_z, *rd_r;               /* [nz], [nr]  the reference's 1-D profiles                */
+    double *tt_r;                     /* [nr]        optional                                    */
+    double *a_rz;                     /* [nr * nz]   optional                                    */
+    double *rd_ra, *tt_ra;            /* [nr * na]   optional                                    */
+    uint64_t *raw;                    /* [tally_words] optional: the fixed-point tally buffer    */
+    double specular;                  /* out: specular reflectance, computed in double           */
+    double kernel_seconds;            /* out: device time of the walk and its reduction          */
+    double wall_seconds;              /* out: host time of the whole call                        */
+    char device[128];                 /* out: "NVIDIA B200 (sm_100)"                            */
+} tmc_result;
+
+/* Fixed-point scale of the tallies: a weight w is added as round(w * 2^32) into an unsigned
+ * 64-bit integer, so every sum is exact and independent of scheduling. */
+#define TMC_B200_FIXED_SCALE 4294967296.0
+
+/* Largest photon count per run. A single tally word holds at most 2^32 launched packets' weight
+ * (2^64 / 2^32); with the roulette's weight boost the headroom is kept at a factor of two. */
+#define TMC_B200_MAX_PHOTONS (1ull << 31)
+
+/* 1 if a CUDA device is present and usable (replaces tissuemc::cuda_available,
+ * include/tissuemc/cuda_engine.hpp:9-11). */
+TMC_B200_API int tmc_b200_available(void);
+
+/* ABI version and the library's build string. */
+TMC_B200_API int tmc_b200_abi_version(void);
+TMC_B200_API const char *tmc_b200_version(void);
+
+/* Options with the reference's defaults (seed 1, 10 batches, rung 0, profiles on; cpu_engine.hpp). */
+TMC_B200_API void tmc_b200_default_options(tmc_options *opt);
+
+/* Validate the run and options exactly as run_cuda does (include/tissuemc/config.hpp:38-66 and
+ * src/cuda/engine.cu:322-350) and report every buffer size. No device is touched. */
+TMC_B200_API int tmc_b200_query_sizes(const tmc_run_spec *spec, const tmc_options *opt, tmc_sizes *sizes,
+                         tmc_status *status);
+
+/* Run the photon walk on the GPU (replaces tissuemc::run_cuda, src/cuda/engine.cu:322-358). */
+TMC_B200_API int tmc_b200_run(const tmc_run_spec *spec, const tmc_options *opt, tmc_result *result,
+                 tmc_status *status);
+
+/* Device-resident variant for callers that keep the tallies on the GPU: zeroes the fixed-point
+ * tally buffer `d_tally` (device memory, tally_words 64-bit words), runs the walk on `stream`
+ * (a cudaStream_t, NULL = the legacy default stream) and returns without synchronising.
+ * `kernel_ms` (optional, host) receives nothing here; time with events on `stream`. */
+TMC_B200_API int tmc_b200_run_device(const tmc_run_spec *spec, const tmc_options *opt, uint64_t *d_tally,
+                        void *stream, tmc_status *status);
+
+/* Convert a raw fixed-point tally buffer (as returned in tmc_result.raw or copied back from
+ * tmc_b200_run_device) into the result arrays; pure host code. */
+TMC_B200_API int tmc_b200_decode(const tmc_run_spec *spec, const tmc_options *opt, const uint64_t *raw,
+                    tmc_result *result, tmc_status *status);
+
+/* Launch and shared-memory plan of a walk: block size, blocks per SM, grid, the shared tiles of
+ * A(r,z) (core rows tr_a x depth bins tz_a, plus the clamped last row and column when cross = 1),
+ * the shared rows of R_d(r,a) and T_t(r,a), whether the per-batch totals are in shared memory, and
+ * the dynamic shared memory per block in bytes. */
+typedef struct {
+    int32_t threads, blocks_per_sm, grid, tr_a, tz_a, cross, tr_rd, tr_tt, batch_smem, smem_bytes;
+} tmc_plan;
+
+/* The plan tmc_b200_run would use on a device with these limits (cudaDeviceProp's
+ * multiProcessorCount, sharedMemPerMultiprocessor, sharedMemPerBlockOptin,
+ * reservedSharedMemPerBlock) when the register limit allows regs_blocks_per_sm blocks per SM.
+ * Pure host code; no device is touched. */
+TMC_B200_API int tmc_b200_plan(const tmc_run_spec *spec, const tmc_options *opt, int32_t sms, int64_t smem_per_sm,
+                  int64_t smem_per_block_optin, int64_t reserved_per_block, int32_t regs_blocks_per_sm,
+                  tmc_plan *plan, tmc_status *status);
+
+/* Parse an MCML .mci file (the reference's parse_mci_file, src/io/mci.cpp:173-183): writes up to
+ * `max_runs` runs and returns the number found in *n_runs. Errors carry the line number. */
+TMC_B200_API int tmc_b200_parse_mci(const char *path, tmc_run_spec *runs, int32_t max_runs, int32_t *n_runs,
+                       tmc_status *status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TISSUEMC_B200_H */

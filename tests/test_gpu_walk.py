@@ -1,0 +1,275 @@
+"""Parity of the B200 walk with the oracle and the reference's own outputs (needs a GPU).
+
+Gates (tests/gates.py): on identical photons (same seed and batches) the GPU's float32 transport
+must meet the reference's cross-engine limits against the float32 CPU path; against the float64 CPU
+engine every total and every profile bin with at least FLOOR contributing scores must have
+|z| < 3; energy is conserved to 3 SE + 1e-6; no anomalies; integer tallies make runs bitwise
+reproducible and independent of the batching.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+import tissuemc_b200 as tmc
+from gates import (batch_estimate, bin_z_scores, compare, conservation, from_engine, from_oracle,
+                   from_reference_json, identical_photon_gaps)
+
+pytestmark = pytest.mark.gpu
+
+FLOOR = 1000  # contributing scores per bin for the per-bin |z| test
+
+
+def _ospec(s: tmc.RunSpec) -> oracle.Spec:
+    return oracle.Spec(layers=list(s.layers), dz=s.dz, dr=s.dr, nz=s.nz, nr=s.nr, na=s.na,
+                       n_above=s.n_above, n_below=s.n_below)
+
+
+def _assert_gaps(gaps):
+    bad = [str(g) for g in gaps if not g.passed]
+    assert not bad, "\n".join(bad)
+
+
+@pytest.fixture(scope="module")
+def slab():
+    return tmc.workload("slab_n14")
+
+
+@pytest.fixture(scope="module")
+def slab_gpu(slab):
+    return tmc.run(slab, photons=1_000_000, batches=80, seed=1)
+
+
+def test_slab_identical_photons_vs_reference_float32(golden, slab_gpu):
+    """cfg 'slab_n14' at its full 1e6 photons vs the reference CPU engine's float32 run."""
+    ref = from_reference_json(golden["runs"]["slab_n14_full/float32"]["result"])
+    _assert_gaps(identical_photon_gaps(ref, from_engine(slab_gpu), profiles=("a_z", "rd_r")))
+
+
+def test_slab_identical_photons_vs_oracle_float32_2d(slab, slab_gpu):
+    o = oracle.run(_ospec(slab), 1_000_000, 80, 1, 32, threads=0)
+    _assert_gaps(identical_photon_gaps(from_oracle(o), from_engine(slab_gpu)))
+
+
+def test_slab_vs_float64_engine_z_below_3(golden, slab, slab_gpu):
+    ref = golden["runs"]["slab_n14_full/float64"]["result"]
+    r = from_reference_json(ref)
+    g = from_engine(slab_gpu)
+    for key in ("rd", "tt", "absorbed"):
+        m_ref, se_ref = batch_estimate(getattr(r, key), r.photons)
+        m, se = batch_estimate(getattr(g, key), g.photons)
+        z, ok = compare(m, se, m_ref, se_ref)
+        assert ok and abs(z) < 3, (key, m, m_ref, z)
+    o = oracle.run(_ospec(slab), 1_000_000, 80, 1, 64, threads=0, counts=True, per_batch_bins=True)
+    for name, ours, ref_t, ref_b, cnt in (
+        ("a_rz", slab_gpu.a_rz, o.a_rz, o.b_a_rz, o.n_a_rz),
+        ("rd_ra", slab_gpu.rd_ra, o.rd_ra, o.b_rd_ra, o.n_rd_ra),
+        ("tt_ra", slab_gpu.tt_ra, o.tt_ra, o.b_tt_ra, o.n_tt_ra),
+    ):
+        z, n = bin_z_scores(ours.ravel(), ref_t.ravel(), ref_b.reshape(ref_b.shape[0], -1), cnt.ravel(), FLOOR)
+        assert n > 0
+        assert z.max() < 3, (name, float(z.max()), n)
+
+
+def test_slab_conservation_and_anomalies(slab_gpu):
+    resid, se, ok = conservation(from_engine(slab_gpu))
+    assert ok, (resid, se)
+    assert int(slab_gpu.anomalies.sum()) == 0
+
+
+def test_profiles_are_projections_of_the_2d_tallies(slab_gpu):
+    r = slab_gpu
+    assert np.array_equal(r.a_z, r.a_rz.sum(axis=0)) or np.allclose(r.a_z, r.a_rz.sum(axis=0), rtol=1e-15)
+    assert math.isclose(r.rd_r.sum(), r.rd.sum(), rel_tol=1e-12)
+    assert math.isclose(r.tt_r.sum(), r.tt.sum(), rel_tol=1e-12)
+    assert math.isclose(r.a_z.sum(), r.absorbed.sum(), rel_tol=1e-12)
+
+
+def test_runs_are_bitwise_reproducible(slab):
+    a = tmc.run(slab, photons=200_000, batches=10, seed=5)
+    b = tmc.run(slab, photons=200_000, batches=10, seed=5)
+    assert np.array_equal(a.raw, b.raw)
+    c = tmc.run(slab, photons=200_000, batches=10, seed=6)
+    assert not np.array_equal(a.raw, c.raw)
+
+
+def test_profiles_do_not_depend_on_batching(slab):
+    a = tmc.run(slab, photons=100_003, batches=1, seed=3)
+    b = tmc.run(slab, photons=100_003, batches=7, seed=3)
+    # integer tallies: the same photons give the same sums, whatever the batches
+    assert np.array_equal(a.raw[-(a.a_rz.size + 2 * a.rd_ra.size):], b.raw[-(b.a_rz.size + 2 * b.rd_ra.size):])
+    assert int(a.events.sum()) == int(b.events.sum())
+    assert b.photons.tolist() == oracle.batch_sizes(100_003, 7).tolist()
+    assert list(b.first_photon) == list(np.cumsum([0] + list(b.photons[:-1])))
+
+
+def test_exact_math_variant_passes_the_same_gates(slab):
+    g = tmc.run(slab, photons=300_000, batches=20, seed=2, fast_math=False)
+    o = oracle.run(_ospec(slab), 300_000, 20, 2, 32, threads=0)
+    _assert_gaps(identical_photon_gaps(from_oracle(o), from_engine(g)))
+
+
+def test_profiles_off_diagnostic_keeps_totals(slab):
+    a = tmc.run(slab, photons=50_000, batches=5, seed=9, rung=6)
+    b = tmc.run(slab, photons=50_000, batches=5, seed=9, rung=6, profiles=False)
+    assert np.array_equal(a.rd, b.rd) and np.array_equal(a.tt, b.tt) and np.array_equal(a.absorbed, b.absorbed)
+    assert np.array_equal(a.events, b.events)
+    assert not b.a_rz.any() and not b.rd_ra.any() and not b.a_z.any()
+
+
+def test_run_device_then_decode_equals_run(slab):
+    torch = pytest.importorskip("torch")
+    opt = tmc.options(photons=30_000, batches=3, seed=4)
+    words = int(tmc.query_sizes(slab, opt).tally_words)
+    buf = torch.empty(words, dtype=torch.int64, device="cuda:0")
+    stream = torch.cuda.current_stream()
+    tmc.run_device(slab, opt, buf.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    raw = buf.cpu().numpy().view(np.uint64)
+    dec = tmc.decode(slab, opt, raw)
+    ref = tmc.run(slab, opt)
+    assert np.array_equal(dec.raw, ref.raw)
+
+
+# ---------------------------------------------------------------- edge cases and other media
+def _parity(spec: tmc.RunSpec, photons: int, batches: int, seed: int, profiles=("a_z", "rd_r", "tt_r")):
+    g = tmc.run(spec, photons=photons, batches=batches, seed=seed)
+    o = oracle.run(_ospec(spec), photons, batches, seed, 32, threads=0)
+    return g, o, identical_photon_gaps(from_oracle(o), from_engine(g), profiles=profiles)
+
+
+def test_single_photon_and_one_photon_per_batch(slab):
+    g = tmc.run(slab, photons=1, batches=1, seed=1)
+    o = oracle.run(_ospec(slab), 1, 1, 1, 32, threads=1)
+    assert int(g.events[0]) == int(o.events[0])
+    g = tmc.run(slab, photons=37, batches=37, seed=1)
+    o = oracle.run(_ospec(slab), 37, 37, 1, 32, threads=1)
+    assert g.photons.tolist() == [1] * 37
+    assert abs(int(g.events.sum()) - int(o.events.sum())) <= 2
+
+
+def test_single_bin_grid():
+    spec = tmc.RunSpec(layers=[(1.37, 1, 100, 0.9, 0.1), (1.37, 1, 10, 0, 0.1), (1.37, 2, 10, 0.7, 0.2)],
+                       dz=0.01, dr=0.01, nz=1, nr=1, na=1)
+    g, o, gaps = _parity(spec, 100_000, 10, 1)
+    _assert_gaps(gaps)
+    assert math.isclose(g.a_rz[0, 0], g.absorbed.sum(), rel_tol=1e-12)
+
+
+def test_sixteen_layers_with_mismatched_indices():
+    layers = [(1.3 + 0.02 * i, 0.5 + 0.1 * i, 50 + 5 * i, 0.5 + 0.02 * i, 0.01 + 0.002 * i) for i in range(16)]
+    spec = tmc.RunSpec(layers=layers, dz=0.01, dr=0.01, nz=40, nr=40, na=5, n_above=1.0, n_below=1.2)
+    _, _, gaps = _parity(spec, 100_000, 10, 8)
+    _assert_gaps(gaps)
+
+
+@pytest.mark.parametrize("g_aniso", [0.0, -0.3, 0.95])
+def test_anisotropy_extremes(g_aniso):
+    spec = tmc.RunSpec(layers=[(1.5, 2, 50, g_aniso, 0.05)], dz=0.005, dr=0.005, nz=20, nr=40, na=10)
+    _, _, gaps = _parity(spec, 100_000, 10, 21)
+    _assert_gaps(gaps)
+
+
+def test_absorbing_slab_closed_form():
+    n, mua, d = 1.5, 5.0, 0.1
+    tau = mua * d
+    spec = tmc.RunSpec(layers=[(n, mua, 0.0, 0.0, d)])
+    photons = 1_000_000
+    g = tmc.run(spec, photons=photons, batches=20, seed=99)
+    rsp = 0.04
+    loop = 1 / (1 - 0.04 * 0.04 * math.exp(-2 * tau))
+    t_exact = (1 - rsp) * math.exp(-tau) * 0.96 * loop
+    r_exact = (1 - rsp) * math.exp(-2 * tau) * 0.04 * 0.96 * loop
+
+    def se(x):
+        p = x / (1 - rsp)
+        return (1 - rsp) * math.sqrt(p * (1 - p) / photons)
+
+    assert abs(g.tt.sum() / photons - t_exact) < 5 * se(t_exact)
+    assert abs(g.rd.sum() / photons - r_exact) < 5 * se(r_exact)
+    assert abs((g.rd.sum() + g.tt.sum() + g.absorbed.sum()) / photons + g.specular - 1) < 1e-5
+
+
+@pytest.mark.parametrize("case", ["o1", "v2"])
+def test_semi_infinite_vs_h_function(golden, case):
+    hf = golden["hf"][case]
+    spec = tmc.RunSpec(layers=[(hf["n_medium"], hf["mua"], hf["mus"], 0.0, 1e8)])
+    g = tmc.run(spec, photons=1_000_000, batches=20, seed=11)
+    m, se = batch_estimate(g.rd, g.photons)
+    _, ok = compare(m, se, hf["rd"])
+    assert ok, (m, se, hf["rd"])
+
+
+@pytest.mark.parametrize("case", ["v1_slab", "v3_three_layer"])
+def test_published_validation_values(golden, case):
+    spec = tmc.parse_mci(golden["dir"] / "validation" / f"{case}.mci")[0]
+    photons = 1_000_000
+    g = tmc.run(spec, photons=photons, batches=20, seed=1)
+    est = {"rd": batch_estimate(g.rd, g.photons), "tt": batch_estimate(g.tt, g.photons)}
+    for chk in golden["refs"]["cases"][case]["checks"]:
+        if chk["quantity"] not in est:
+            continue
+        m, se = est[chk["quantity"]]
+        rounding = 0.5 * 10 ** (-chk["decimals"]) if "decimals" in chk else 0.0
+        se_ref = chk.get("se", se * math.sqrt(photons / chk["n_photons"]) if "n_photons" in chk else 0.0)
+        z, ok = compare(m, se, chk["value"], se_ref, rounding)
+        assert ok, (case, chk, m, se, z)
+
+
+# ---------------------------------------------------------------- the five-layer stack (tiled tallies)
+@pytest.fixture(scope="module")
+def skin():
+    return tmc.workload("skin5")
+
+
+def test_skin5_identical_photons_vs_oracle(skin):
+    g, o, gaps = _parity(skin, 200_000, 20, 9, profiles=("a_z", "rd_r", "tt_r", "a_rz", "rd_ra", "tt_ra"))
+    _assert_gaps(gaps)
+
+
+def test_skin5_matches_reference_golden_run(golden, skin):
+    ref = golden["runs"]["skin5/float32"]
+    g = tmc.run(skin, photons=ref["photons"], batches=ref["batches"], seed=ref["seed"])
+    _assert_gaps(identical_photon_gaps(from_reference_json(ref["result"]), from_engine(g), profiles=("a_z", "rd_r")))
+
+
+def test_skin5_full_size_properties(skin):
+    """1e8 photons: conservation, no anomalies, exact projections, bitwise reproducibility."""
+    a = tmc.run(skin, batches=100, seed=1)
+    assert int(a.photons.sum()) == 100_000_000
+    resid, se, ok = conservation(from_engine(a))
+    assert ok, (resid, se)
+    assert int(a.anomalies.sum()) == 0
+    assert math.isclose(a.a_z.sum(), a.absorbed.sum(), rel_tol=1e-12)
+    assert math.isclose(a.rd_r.sum(), a.rd.sum(), rel_tol=1e-12)
+    b = tmc.run(skin, batches=100, seed=1)
+    assert np.array_equal(a.raw, b.raw)
+
+
+def test_skin5_vs_float64_engine_independent_seeds(skin):
+    """Totals against an independent float64 run (different seed): |z| < 3."""
+    g = tmc.run(skin, photons=2_000_000, batches=20, seed=101)
+    o = oracle.run(_ospec(skin), 200_000, 20, 202, 64, threads=0)
+    for key in ("rd", "tt", "absorbed"):
+        sg = getattr(g, key) if key != "absorbed" else g.absorbed.sum(axis=1)
+        so = getattr(o, key) if key != "absorbed" else o.absorbed.sum(axis=1)
+        m, se = batch_estimate(sg, g.photons)
+        mo, seo = batch_estimate(so, o.photons)
+        z, ok = compare(m, se, mo, seo)
+        assert ok, (key, m, mo, z)
+
+
+# ---------------------------------------------------------------- errors
+def test_bad_config_raises_config_error(slab):
+    with pytest.raises(tmc.ConfigError, match="batches cannot exceed the number of photons"):
+        tmc.run(slab, photons=5, batches=6)
+
+
+def test_bad_device_ordinal_is_no_device(slab):
+    with pytest.raises(tmc.EngineError) as e:
+        tmc.run(slab, photons=100, batches=1, device=63)
+    assert e.value.code == tmc.NO_DEVICE

@@ -1,0 +1,385 @@
+"""tissuemc_b200 — a B200 (sm_100a) engine for TissueMC's MCML photon walk.
+
+Python access to the engine's C ABI (include/tissuemc_b200.h) through ctypes. The CUDA kernels,
+the C ABI and the C++ host code (the .mci reader, the run_cuda drop-in, the JSON writer and the
+`tissuemc` CLI) are all in the in-tree library ``libtissuemc_b200.so``; this module only marshals
+arguments. There is no fallback: if the library is missing or no GPU is present, the calls raise.
+
+    import tissuemc_b200 as tmc
+    spec = tmc.parse_mci("tissuemc_b200/configs/slab_n14.mci")[0]
+    res = tmc.run(spec, photons=10**6, batches=10, seed=1)
+    print(res.summary())
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libtissuemc_b200.so"
+CLI_PATH = PKG / "bin" / "tissuemc"
+CONFIGS = PKG / "configs"
+MAX_LAYERS = 16
+FIXED_SCALE = 2.0**32
+
+# status codes (tmc_status_code)
+OK, BAD_CONFIG, NO_DEVICE, CUDA_ERROR, DEVICE_TIMEOUT, BAD_ARGUMENT = range(6)
+
+
+class ConfigError(ValueError):
+    """An invalid run description or options (the reference's tissuemc::ConfigError)."""
+
+
+class EngineError(RuntimeError):
+    """No usable device, a CUDA failure or a device-side timeout."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+# ---------------------------------------------------------------------------------- C structs
+class Layer(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("n", "mua", "mus", "g", "d")]
+
+
+class CRunSpec(ctypes.Structure):
+    _fields_ = [
+        ("photons", ctypes.c_uint64),
+        ("dz", ctypes.c_double),
+        ("dr", ctypes.c_double),
+        ("nz", ctypes.c_int32),
+        ("nr", ctypes.c_int32),
+        ("na", ctypes.c_int32),
+        ("n_above", ctypes.c_double),
+        ("n_below", ctypes.c_double),
+        ("num_layers", ctypes.c_int32),
+        ("layers", Layer * MAX_LAYERS),
+    ]
+
+
+class COptions(ctypes.Structure):
+    _fields_ = [
+        ("seed", ctypes.c_uint64),
+        ("batches", ctypes.c_int32),
+        ("photons", ctypes.c_uint64),
+        ("rung", ctypes.c_int32),
+        ("profiles", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("fast_math", ctypes.c_int32),
+        ("threads_per_block", ctypes.c_int32),
+        ("blocks_per_sm", ctypes.c_int32),
+        ("smem_budget", ctypes.c_int32),
+    ]
+
+
+class CSizes(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in
+                ("batches", "layers", "nz", "nr", "na", "absorbed", "a_rz", "ra", "tally_words")]
+
+
+_pd, _pu = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)
+
+
+class CResult(ctypes.Structure):
+    _fields_ = [
+        ("first_photon", _pu), ("photons", _pu), ("rd", _pd), ("tt", _pd), ("absorbed", _pd),
+        ("events", _pu), ("anomalies", _pu), ("a_z", _pd), ("rd_r", _pd), ("tt_r", _pd),
+        ("a_rz", _pd), ("rd_ra", _pd), ("tt_ra", _pd), ("raw", _pu),
+        ("specular", ctypes.c_double), ("kernel_seconds", ctypes.c_double),
+        ("wall_seconds", ctypes.c_double), ("device", ctypes.c_char * 128),
+    ]  # fmt: skip
+
+
+class CStatus(ctypes.Structure):
+    _fields_ = [("code", ctypes.c_int32), ("message", ctypes.c_char * 512)]
+
+
+class CPlan(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int32) for k in
+                ("threads", "blocks_per_sm", "grid", "tr_a", "tz_a", "cross", "tr_rd", "tr_tt",
+                 "batch_smem", "smem_bytes")]
+
+
+# Every entry point include/tissuemc_b200.h declares: name -> (restype, argtypes)
+_P = ctypes.POINTER
+PROTOTYPES = {
+    "tmc_b200_available": (ctypes.c_int, []),
+    "tmc_b200_abi_version": (ctypes.c_int, []),
+    "tmc_b200_version": (ctypes.c_char_p, []),
+    "tmc_b200_default_options": (None, [_P(COptions)]),
+    "tmc_b200_query_sizes": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _P(CSizes), _P(CStatus)]),
+    "tmc_b200_run": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _P(CResult), _P(CStatus)]),
+    "tmc_b200_run_device": (ctypes.c_int, [_P(CRunSpec), _P(COptions), ctypes.c_void_p,
+                                           ctypes.c_void_p, _P(CStatus)]),
+    "tmc_b200_decode": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _pu, _P(CResult), _P(CStatus)]),
+    "tmc_b200_parse_mci": (ctypes.c_int, [ctypes.c_char_p, _P(CRunSpec), ctypes.c_int32,
+                                          _P(ctypes.c_int32), _P(CStatus)]),
+    "tmc_b200_plan": (ctypes.c_int, [_P(CRunSpec), _P(COptions), ctypes.c_int32, ctypes.c_int64,
+                                     ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _P(CPlan),
+                                     _P(CStatus)]),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded engine library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m tissuemc_b200.build` "
+                "(there is no CPU fallback)"
+            )
+        handle = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in PROTOTYPES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def _check(rc: int, st: CStatus) -> None:
+    if rc == OK:
+        return
+    msg = st.message.decode(errors="replace")
+    if rc == BAD_CONFIG:
+        raise ConfigError(msg)
+    raise EngineError(rc, msg)
+
+
+# ---------------------------------------------------------------------------------- Python API
+@dataclass
+class RunSpec:
+    """One MCML run (the reference's RunSpec): layers are (n, mua, mus, g, d) tuples."""
+
+    layers: list[tuple[float, float, float, float, float]]
+    photons: int = 1000
+    dz: float = 0.01
+    dr: float = 0.01
+    nz: int = 1
+    nr: int = 1
+    na: int = 1
+    n_above: float = 1.0
+    n_below: float = 1.0
+    output_name: str = "run.mco"
+
+    def to_c(self) -> CRunSpec:
+        s = CRunSpec()
+        s.photons, s.dz, s.dr = self.photons, self.dz, self.dr
+        s.nz, s.nr, s.na = self.nz, self.nr, self.na
+        s.n_above, s.n_below = self.n_above, self.n_below
+        s.num_layers = len(self.layers)
+        for i, lay in enumerate(self.layers[:MAX_LAYERS]):
+            s.layers[i] = Layer(*map(float, lay))
+        return s
+
+    @staticmethod
+    def from_c(c: CRunSpec, name: str = "run.mco") -> RunSpec:
+        layers = [(c.layers[i].n, c.layers[i].mua, c.layers[i].mus, c.layers[i].g, c.layers[i].d)
+                  for i in range(c.num_layers)]
+        return RunSpec(layers=layers, photons=c.photons, dz=c.dz, dr=c.dr, nz=c.nz, nr=c.nr,
+                       na=c.na, n_above=c.n_above, n_below=c.n_below, output_name=name)
+
+    def to_mci(self) -> str:
+        rows = ["1.0", "1", f"{self.output_name} A", str(self.photons), f"{self.dz!r} {self.dr!r}",
+                f"{self.nz} {self.nr} {self.na}", str(len(self.layers)), repr(float(self.n_above))]
+        rows += [" ".join(repr(float(v)) for v in lay) for lay in self.layers]
+        rows.append(repr(float(self.n_below)))
+        return "\n".join(rows) + "\n"
+
+
+def options(seed: int = 1, batches: int = 10, photons: int = 0, rung: int = 0, profiles: bool = True,
+            device: int = 0, fast_math: bool = True, threads_per_block: int = 0, blocks_per_sm: int = 0,
+            smem_budget: int = 0) -> COptions:
+    o = COptions()
+    lib().tmc_b200_default_options(ctypes.byref(o))
+    o.seed, o.batches, o.photons, o.rung = seed, batches, photons, rung
+    o.profiles, o.device, o.fast_math = int(profiles), device, int(fast_math)
+    o.threads_per_block, o.blocks_per_sm, o.smem_budget = threads_per_block, blocks_per_sm, smem_budget
+    return o
+
+
+@dataclass
+class Estimate:
+    mean: float
+    se: float
+
+
+def batch_estimate(sums, photons) -> Estimate:
+    """Per-photon mean and its standard error from per-batch sums (src/io/json_out.cpp:37-64)."""
+    sums = np.asarray(sums, dtype=np.float64)
+    photons = np.asarray(photons, dtype=np.float64)
+    mean = float(math.fsum(sums) / photons.sum())
+    n = len(sums)
+    if n < 2:
+        return Estimate(mean, math.nan)
+    per = sums / photons
+    centre = math.fsum(per) / n
+    ss = math.fsum((per - centre) ** 2)
+    return Estimate(mean, math.sqrt(ss / (n - 1) / n))
+
+
+@dataclass
+class RunResult:
+    """Output of one run, in the reference's layout plus the 2-D tallies (numpy arrays)."""
+
+    spec: RunSpec
+    seed: int
+    first_photon: np.ndarray
+    photons: np.ndarray
+    rd: np.ndarray
+    tt: np.ndarray
+    absorbed: np.ndarray  # (batches, layers)
+    events: np.ndarray
+    anomalies: np.ndarray
+    a_z: np.ndarray
+    rd_r: np.ndarray
+    tt_r: np.ndarray
+    a_rz: np.ndarray  # (nr, nz)
+    rd_ra: np.ndarray  # (nr, na)
+    tt_ra: np.ndarray  # (nr, na)
+    raw: np.ndarray
+    specular: float
+    kernel_seconds: float
+    wall_seconds: float
+    device: str
+    rung: int = 0
+    profiles: bool = True
+    extra: dict = field(default_factory=dict)
+
+    def estimate(self, key: str) -> Estimate:
+        if key == "absorbed":
+            return batch_estimate(self.absorbed.sum(axis=1), self.photons)
+        if key == "conservation_residual":
+            e = batch_estimate(self.rd + self.tt + self.absorbed.sum(axis=1), self.photons)
+            return Estimate(e.mean + self.specular - 1.0, e.se)
+        return batch_estimate(getattr(self, key), self.photons)
+
+    def summary(self) -> dict:
+        return {k: self.estimate(k).__dict__ for k in ("rd", "tt", "absorbed", "conservation_residual")}
+
+    def to_json(self) -> dict:
+        """The result as the reference's JSON run object (src/io/json_out.cpp:164-306) plus the
+        2-D arrays."""
+        s = self.spec
+        return {
+            "tissuemc_version": "0.1.0", "engine": "cuda", "precision": "float32", "seed": self.seed,
+            "threads": 1, "photons": int(self.photons.sum()), "output_name": s.output_name,
+            "n_above": s.n_above, "n_below": s.n_below,
+            "layers": [dict(zip(("n", "mua", "mus", "g", "d"), lay, strict=True)) for lay in s.layers],
+            "grid": {"dz": s.dz, "dr": s.dr, "nz": s.nz, "nr": s.nr, "na": s.na},
+            "specular": self.specular, "wall_seconds": self.wall_seconds,
+            "kernel_seconds": self.kernel_seconds, "device": self.device,
+            "tally_precision": "fixed64", "rung": self.rung, "profiles": self.profiles,
+            "events": int(self.events.sum()), "anomalies": int(self.anomalies.sum()),
+            "summary": self.summary(),
+            "batches": [
+                {"first_photon": int(self.first_photon[b]), "photons": int(self.photons[b]),
+                 "rd": float(self.rd[b]), "tt": float(self.tt[b]),
+                 "absorbed": [float(v) for v in self.absorbed[b]], "events": int(self.events[b]),
+                 "anomalies": int(self.anomalies[b])}
+                for b in range(len(self.rd))
+            ],
+            "a_z": self.a_z.tolist(), "rd_r": self.rd_r.tolist(), "tt_r": self.tt_r.tolist(),
+            "a_rz": self.a_rz.tolist(), "rd_ra": self.rd_ra.tolist(), "tt_ra": self.tt_ra.tolist(),
+        }  # fmt: skip
+
+
+def available() -> bool:
+    return bool(lib().tmc_b200_available())
+
+
+def query_sizes(spec: RunSpec, opt: COptions) -> CSizes:
+    sz, st = CSizes(), CStatus()
+    c = spec.to_c()
+    _check(lib().tmc_b200_query_sizes(ctypes.byref(c), ctypes.byref(opt), ctypes.byref(sz), ctypes.byref(st)), st)
+    return sz
+
+
+def _alloc_result(sz: CSizes):
+    b, nz, nr, na = int(sz.batches), int(sz.nz), int(sz.nr), int(sz.na)
+    arrs = {
+        "first_photon": np.zeros(b, np.uint64), "photons": np.zeros(b, np.uint64),
+        "rd": np.zeros(b), "tt": np.zeros(b), "absorbed": np.zeros((b, int(sz.layers))),
+        "events": np.zeros(b, np.uint64), "anomalies": np.zeros(b, np.uint64),
+        "a_z": np.zeros(nz), "rd_r": np.zeros(nr), "tt_r": np.zeros(nr),
+        "a_rz": np.zeros((nr, nz)), "rd_ra": np.zeros((nr, na)), "tt_ra": np.zeros((nr, na)),
+        "raw": np.zeros(int(sz.tally_words), np.uint64),
+    }  # fmt: skip
+    res = CResult()
+    for k, a in arrs.items():
+        ct = ctypes.c_uint64 if a.dtype == np.uint64 else ctypes.c_double
+        setattr(res, k, a.ctypes.data_as(ctypes.POINTER(ct)))
+    return arrs, res
+
+
+def run(spec: RunSpec, opt: COptions | None = None, **kw) -> RunResult:
+    """Run the photon walk on the GPU (the reference's run_cuda). Keyword arguments build the
+    options when `opt` is not given (see `options`)."""
+    if opt is None:
+        opt = options(**kw)
+    sz = query_sizes(spec, opt)
+    arrs, res = _alloc_result(sz)
+    st = CStatus()
+    c = spec.to_c()
+    _check(lib().tmc_b200_run(ctypes.byref(c), ctypes.byref(opt), ctypes.byref(res), ctypes.byref(st)), st)
+    return RunResult(spec=spec, seed=opt.seed, specular=res.specular, kernel_seconds=res.kernel_seconds,
+                     wall_seconds=res.wall_seconds, device=res.device.decode(), rung=opt.rung,
+                     profiles=bool(opt.profiles), **arrs)
+
+
+def decode(spec: RunSpec, opt: COptions, raw: np.ndarray) -> RunResult:
+    """Decode a raw fixed-point tally buffer (from run_device) into a RunResult."""
+    sz = query_sizes(spec, opt)
+    arrs, res = _alloc_result(sz)
+    raw = np.ascontiguousarray(raw, dtype=np.uint64)
+    st = CStatus()
+    c = spec.to_c()
+    _check(lib().tmc_b200_decode(ctypes.byref(c), ctypes.byref(opt),
+                                 raw.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                 ctypes.byref(res), ctypes.byref(st)), st)
+    return RunResult(spec=spec, seed=opt.seed, specular=res.specular, kernel_seconds=0.0,
+                     wall_seconds=0.0, device="", rung=opt.rung, profiles=bool(opt.profiles), **arrs)
+
+
+def run_device(spec: RunSpec, opt: COptions, d_tally_ptr: int, stream_ptr: int = 0) -> None:
+    """Launch the walk into a device tally buffer on a stream, without synchronising."""
+    st = CStatus()
+    c = spec.to_c()
+    _check(lib().tmc_b200_run_device(ctypes.byref(c), ctypes.byref(opt), ctypes.c_void_p(d_tally_ptr),
+                                     ctypes.c_void_p(stream_ptr), ctypes.byref(st)), st)
+
+
+def plan(spec: RunSpec, opt: COptions, sms: int = 148, smem_sm: int = 233472,
+         smem_block_optin: int = 232448, reserved: int = 1024, regs_blocks_per_sm: int = 4) -> CPlan:
+    """The launch and shared-memory tile plan the engine would use on a device with these limits
+    (pure host code)."""
+    p, st = CPlan(), CStatus()
+    c = spec.to_c()
+    _check(lib().tmc_b200_plan(ctypes.byref(c), ctypes.byref(opt), sms, smem_sm, smem_block_optin,
+                               reserved, regs_blocks_per_sm, ctypes.byref(p), ctypes.byref(st)), st)
+    return p
+
+
+def parse_mci(path: str | Path) -> list[RunSpec]:
+    """Read an MCML .mci file with the engine's C++ reader (errors carry line numbers)."""
+    runs = (CRunSpec * 64)()
+    n = ctypes.c_int32(0)
+    st = CStatus()
+    _check(lib().tmc_b200_parse_mci(str(path).encode(), runs, 64, ctypes.byref(n), ctypes.byref(st)), st)
+    if n.value > 64:
+        raise ConfigError(f"{path}: more than 64 runs")
+    return [RunSpec.from_c(runs[i], name=Path(path).stem + ".mco") for i in range(n.value)]
+
+
+def workload(name: str) -> RunSpec:
+    """A bundled workload: 'slab_n14' (one slab, 1e6 photons) or 'skin5' (five layers, 1e8)."""
+    return parse_mci(CONFIGS / f"{name}.mci")[0]

@@ -1,0 +1,397 @@
+// Host driver and C ABI of the B200 photon-walk engine (include/tissuemc_b200.h).
+//
+// Replaces TissueMC's src/cuda/engine.cu:322-358 (run_cuda) and :193-313 (run_with_tallies):
+// the same validation and error texts, one persistent launch of walk_kernel, integer tallies
+// decoded into the reference's result layout plus the 2-D arrays.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tissuemc_b200.h"
+#include "walk_kernel.cuh"
+#include "engine_host.hpp"
+
+namespace tmc {
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+
+class Fail : public std::runtime_error {
+  public:
+    Fail(int code, const std::string &msg) : std::runtime_error(msg), code_(code) {}
+    int code() const { return code_; }
+
+  private:
+    int code_;
+};
+
+#define TMC_CUDA(call)                                                                              \
+    do {                                                                                            \
+        const cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                      \
+            throw Fail(TMC_CUDA_ERROR, std::string("CUDA error at ") + __FILE__ + ":" +             \
+                                           std::to_string(__LINE__) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Per-device state kept across calls: a stream, timing events, the tally buffer, the claim
+// counter and a pinned staging buffer. Grown on demand, never shrunk.
+struct DeviceCtx {
+    bool ready = false;
+    cudaDeviceProp prop{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    unsigned long long *d_tally = nullptr;
+    size_t tally_cap = 0;  // words
+    unsigned long long *d_counter = nullptr;
+    uint64_t *h_stage = nullptr;
+    size_t stage_cap = 0;  // words
+};
+
+DeviceCtx g_ctx[kMaxDevices];
+std::mutex g_mu;
+
+void set_status(tmc_status *st, int code, const std::string &msg) {
+    if (!st) return;
+    st->code = code;
+    std::snprintf(st->message, sizeof st->message, "%s", msg.c_str());
+}
+
+DeviceCtx &device_ctx(int dev) {
+    if (dev < 0 || dev >= kMaxDevices) throw Fail(TMC_BAD_CONFIG, "device ordinal out of range");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        throw Fail(TMC_NO_DEVICE, "no usable CUDA device found");
+    }
+    if (dev >= n) throw Fail(TMC_NO_DEVICE, "no usable CUDA device found");
+    TMC_CUDA(cudaSetDevice(dev));
+    DeviceCtx &c = g_ctx[dev];
+    if (!c.ready) {
+        TMC_CUDA(cudaGetDeviceProperties(&c.prop, dev));
+        TMC_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+        TMC_CUDA(cudaEventCreate(&c.ev0));
+        TMC_CUDA(cudaEventCreate(&c.ev1));
+        TMC_CUDA(cudaMalloc(&c.d_counter, 64));
+        TMC_CUDA(cudaFuncSetAttribute(walk_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      c.prop.sharedMemPerBlockOptin));
+        TMC_CUDA(cudaFuncSetAttribute(walk_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      c.prop.sharedMemPerBlockOptin));
+        c.ready = true;
+    }
+    return c;
+}
+
+DeviceLimits limits_of(const cudaDeviceProp &p) {
+    return DeviceLimits{p.multiProcessorCount, p.sharedMemPerMultiprocessor, p.sharedMemPerBlockOptin,
+                        p.reservedSharedMemPerBlock};
+}
+
+void ensure_tally(DeviceCtx &c, size_t words) {
+    if (words <= c.tally_cap) return;
+    if (c.d_tally) TMC_CUDA(cudaFree(c.d_tally));
+    c.d_tally = nullptr;
+    c.tally_cap = 0;
+    TMC_CUDA(cudaMalloc(&c.d_tally, words * 8));
+    c.tally_cap = words;
+}
+
+void ensure_stage(DeviceCtx &c, size_t words) {
+    if (words <= c.stage_cap) return;
+    if (c.h_stage) TMC_CUDA(cudaFreeHost(c.h_stage));
+    c.h_stage = nullptr;
+    c.stage_cap = 0;
+    TMC_CUDA(cudaMallocHost(&c.h_stage, words * 8));
+    c.stage_cap = words;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------ planning
+// Shared-memory plan: the layer table, then (if they fit in a quarter of the budget) the per-batch
+// totals, then the profile tallies. When the whole of A(r,z), R_d(r,a) and T_t(r,a) fits, all of it
+// is privatised; otherwise R_d and T_t get the first rows (exits concentrate near the axis) and
+// A(r,z) a core tile plus its clamped last row and column (the bins that collect every deposit
+// beyond the grid, the hottest of a deep or wide stack). Everything else goes to global atomics.
+Plan make_plan(const tmc_run_spec &spec, const tmc_options &opt, const DeviceLimits &lim,
+               int regs_blocks_per_sm) {
+    Plan p{};
+    const RunShape sh = shape_of(spec, opt);
+    p.threads = opt.threads_per_block > 0 ? opt.threads_per_block : 256;
+    const int bps = opt.blocks_per_sm > 0 ? opt.blocks_per_sm : std::max(1, regs_blocks_per_sm);
+    p.blocks_per_sm = bps;
+    size_t budget = opt.smem_budget > 0
+                        ? static_cast<size_t>(opt.smem_budget)
+                        : std::min(lim.smem_block_optin, lim.smem_sm / static_cast<size_t>(bps) - lim.reserved);
+    budget &= ~static_cast<size_t>(15);
+    const size_t layer_bytes = ((static_cast<size_t>(sh.nl) * sizeof(LayerC) + 15) / 16) * 16;
+    size_t rem = budget > layer_bytes + 16 ? budget - layer_bytes - 16 : 0;
+    const size_t batch_bytes = static_cast<size_t>(sh.nb) * (4 + sh.nl) * 8;
+    p.batch_smem = batch_bytes <= rem / 4 ? 1 : 0;
+    if (p.batch_smem) rem -= batch_bytes;
+    const size_t nr = sh.nr, nz = sh.nz, na = sh.na;
+    if (opt.profiles) {
+        const size_t full_a = nr * nz * 8, full_ra = nr * na * 8;
+        if (full_a + 2 * full_ra <= rem) {
+            p.tr_a = sh.nr;
+            p.tz_a = sh.nz;
+            p.tr_rd = p.tr_tt = sh.nr;
+        } else {
+            const size_t ra_each = std::min(full_ra, rem / 8);
+            p.tr_rd = p.tr_tt = static_cast<int>(ra_each / (na * 8));
+            rem -= 2 * static_cast<size_t>(p.tr_rd) * na * 8;
+            const size_t cross = (nr + nz) * 8;
+            if (rem >= cross) {
+                p.cross = 1;
+                const size_t core = (rem - cross) / 8;
+                size_t tz = std::min<size_t>(nz - 1, static_cast<size_t>(2.0 * std::sqrt(static_cast<double>(core))));
+                size_t tr = tz > 0 ? std::min<size_t>(nr - 1, core / tz) : 0;
+                if (tr == 0 || tz == 0) tr = tz = 0;
+                p.tr_a = static_cast<int>(tr);
+                p.tz_a = static_cast<int>(tz);
+            }
+        }
+    }
+    p.grid = lim.sms * bps;
+    return p;
+}
+
+size_t plan_smem_bytes(const WalkParams &P) { return static_cast<size_t>(smem_layout(P).total) * 8; }
+
+// Fill WalkParams from a validated run (layers in float, computed as the reference does).
+WalkParams make_params(const tmc_run_spec &spec, const tmc_options &opt, const Plan &pl,
+                       unsigned long long *d_tally, unsigned long long *d_counter) {
+    const RunShape sh = shape_of(spec, opt);
+    WalkParams P{};
+    P.photons = sh.photons;
+    P.seed = opt.seed;
+    P.plan_base = sh.photons / static_cast<uint64_t>(sh.nb);
+    P.plan_extra = sh.photons % static_cast<uint64_t>(sh.nb);
+    P.nb = sh.nb;
+    P.nl = sh.nl;
+    P.nz = sh.nz;
+    P.nr = sh.nr;
+    P.na = sh.na;
+    const TallyOffsets off = tally_offsets(sh);
+    P.counter = d_counter;
+    P.g_batch = d_tally + off.batch;
+    P.g_arz = d_tally + off.a_rz;
+    P.g_rd = d_tally + off.rd_ra;
+    P.g_tt = d_tally + off.tt_ra;
+    {
+        const float n0 = static_cast<float>(spec.n_above), n1 = static_cast<float>(spec.layers[0].n);
+        const float r = (n0 - n1) / (n0 + n1);
+        P.launch_w = 1.0f - r * r;
+    }
+    P.dz = static_cast<float>(spec.dz);
+    P.dr = static_cast<float>(spec.dr);
+    P.da = static_cast<float>(0.5 * 3.14159265358979323846 / spec.na);
+    P.inv_dz = 1.0f / P.dz;
+    P.inv_dr = 1.0f / P.dr;
+    P.inv_da = 1.0f / P.da;
+    P.tr_a = pl.tr_a;
+    P.tz_a = pl.tz_a;
+    P.tr_rd = pl.tr_rd;
+    P.tr_tt = pl.tr_tt;
+    P.cross = pl.cross;
+    P.batch_smem = pl.batch_smem;
+    P.profiles = opt.profiles ? 1 : 0;
+    P.step_cap = 2000000000u;
+    P.chunk = 256;
+    double zacc = 0.0;
+    for (int i = 0; i < sh.nl; ++i) {
+        const tmc_layer &s = spec.layers[i];
+        const double nt = i == 0 ? spec.n_above : spec.layers[i - 1].n;
+        const double nb = i + 1 == sh.nl ? spec.n_below : spec.layers[i + 1].n;
+        LayerC &L = P.layers[i];
+        L.mua = static_cast<float>(s.mua);
+        L.mus = static_cast<float>(s.mus);
+        L.mut = L.mua + L.mus;
+        L.inv_mut = 1.0f / L.mut;
+        L.absorb = L.mua / L.mut;
+        L.z0 = static_cast<float>(zacc);
+        zacc += s.d;
+        L.z1 = static_cast<float>(zacc);
+        L.g = static_cast<float>(s.g);
+        L.hg_a = 1.0f - L.g * L.g;
+        L.hg_b = 1.0f - L.g;
+        L.hg_c = 2.0f * L.g;
+        L.hg_d = 1.0f + L.g * L.g;
+        L.inv_2g = L.g != 0.0f ? 1.0f / (2.0f * L.g) : 0.0f;
+        L.n = static_cast<float>(s.n);
+        L.n_up = static_cast<float>(nt);
+        L.n_dn = static_cast<float>(nb);
+        L.cc_up = static_cast<float>(s.n > nt ? std::sqrt(1.0 - (nt * nt) / (s.n * s.n)) : 0.0);
+        L.cc_dn = static_cast<float>(s.n > nb ? std::sqrt(1.0 - (nb * nb) / (s.n * s.n)) : 0.0);
+        L.rat_up = L.n / L.n_up;
+        L.rat_dn = L.n / L.n_dn;
+        {
+            const float r = (L.n_up - L.n) / (L.n_up + L.n);
+            L.rn_up = r * r;
+        }
+        {
+            const float r = (L.n_dn - L.n) / (L.n_dn + L.n);
+            L.rn_dn = r * r;
+        }
+    }
+    return P;
+}
+
+namespace {
+
+// Launch the walk on `stream` into `d_tally` (zeroed here). Records ev0/ev1 around it if given.
+void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
+                 unsigned long long *d_tally, cudaStream_t stream, cudaEvent_t e0, cudaEvent_t e1) {
+    const RunShape sh = shape_of(spec, opt);
+    const size_t words = tally_offsets(sh).total;
+    int regs_bps = 0;
+    const int threads = opt.threads_per_block > 0 ? opt.threads_per_block : 256;
+    if (opt.fast_math)
+        TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&regs_bps, walk_kernel<1>, threads, 0));
+    else
+        TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&regs_bps, walk_kernel<0>, threads, 0));
+    const Plan pl = make_plan(spec, opt, limits_of(c.prop), regs_bps);
+    WalkParams P = make_params(spec, opt, pl, d_tally, c.d_counter);
+    const size_t smem = plan_smem_bytes(P);
+    if (smem > c.prop.sharedMemPerBlockOptin)
+        throw Fail(TMC_BAD_CONFIG, "the tally plan does not fit in shared memory");
+    // never more lanes than photons: whole blocks only
+    const uint64_t max_blocks = (sh.photons + pl.threads - 1) / pl.threads;
+    const int grid = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(pl.grid), max_blocks));
+    if (e0) TMC_CUDA(cudaEventRecord(e0, stream));
+    TMC_CUDA(cudaMemsetAsync(d_tally, 0, words * 8, stream));
+    TMC_CUDA(cudaMemsetAsync(c.d_counter, 0, 8, stream));
+    if (opt.fast_math)
+        walk_kernel<1><<<grid, pl.threads, smem, stream>>>(P);
+    else
+        walk_kernel<0><<<grid, pl.threads, smem, stream>>>(P);
+    TMC_CUDA(cudaGetLastError());
+    if (e1) TMC_CUDA(cudaEventRecord(e1, stream));
+}
+
+}  // namespace
+}  // namespace tmc
+
+// ================================================================================== C ABI
+using namespace tmc;
+
+extern "C" {
+
+int tmc_b200_available(void) {
+    int n = 0;
+    const bool ok = cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
+    if (!ok) cudaGetLastError();
+    return ok ? 1 : 0;
+}
+
+int tmc_b200_abi_version(void) { return TMC_B200_ABI_VERSION; }
+
+const char *tmc_b200_version(void) { return "tissuemc-b200 0.1.0 (sm_100a)"; }
+
+int tmc_b200_run(const tmc_run_spec *spec, const tmc_options *opt, tmc_result *res, tmc_status *st) {
+    set_status(st, TMC_OK, "");
+    if (!spec || !opt || !res) {
+        set_status(st, TMC_BAD_ARGUMENT, "NULL argument");
+        return TMC_BAD_ARGUMENT;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    std::lock_guard<std::mutex> lock(g_mu);
+    try {
+        validate_run(*spec, *opt);  // throws Fail-compatible ConfigFailure
+        const RunShape sh = shape_of(*spec, *opt);
+        const size_t words = tally_offsets(sh).total;
+        DeviceCtx &c = device_ctx(opt->device);
+        ensure_tally(c, words);
+        ensure_stage(c, words);
+        launch_walk(*spec, *opt, c, c.d_tally, c.stream, c.ev0, c.ev1);
+        TMC_CUDA(cudaMemcpyAsync(c.h_stage, c.d_tally, words * 8, cudaMemcpyDeviceToHost, c.stream));
+        TMC_CUDA(cudaStreamSynchronize(c.stream));
+        float ms = 0.f;
+        TMC_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+        decode_tallies(*spec, *opt, c.h_stage, *res);
+        res->kernel_seconds = static_cast<double>(ms) / 1000.0;
+        std::snprintf(res->device, sizeof res->device, "%.100s (sm_%d%d)", c.prop.name, c.prop.major,
+                      c.prop.minor);
+        res->wall_seconds =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return TMC_OK;
+    } catch (const ConfigFailure &e) {
+        set_status(st, TMC_BAD_CONFIG, e.what());
+        return TMC_BAD_CONFIG;
+    } catch (const Fail &e) {
+        set_status(st, e.code(), e.what());
+        return e.code();
+    } catch (const std::exception &e) {
+        set_status(st, TMC_CUDA_ERROR, e.what());
+        return TMC_CUDA_ERROR;
+    }
+}
+
+int tmc_b200_run_device(const tmc_run_spec *spec, const tmc_options *opt, uint64_t *d_tally,
+                        void *stream, tmc_status *st) {
+    set_status(st, TMC_OK, "");
+    if (!spec || !opt || !d_tally) {
+        set_status(st, TMC_BAD_ARGUMENT, "NULL argument");
+        return TMC_BAD_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    try {
+        validate_run(*spec, *opt);
+        DeviceCtx &c = device_ctx(opt->device);
+        launch_walk(*spec, *opt, c, reinterpret_cast<unsigned long long *>(d_tally),
+                    static_cast<cudaStream_t>(stream), nullptr, nullptr);
+        return TMC_OK;
+    } catch (const ConfigFailure &e) {
+        set_status(st, TMC_BAD_CONFIG, e.what());
+        return TMC_BAD_CONFIG;
+    } catch (const Fail &e) {
+        set_status(st, e.code(), e.what());
+        return e.code();
+    } catch (const std::exception &e) {
+        set_status(st, TMC_CUDA_ERROR, e.what());
+        return TMC_CUDA_ERROR;
+    }
+}
+
+int tmc_b200_plan(const tmc_run_spec *spec, const tmc_options *opt, int32_t sms, int64_t smem_per_sm,
+                  int64_t smem_per_block_optin, int64_t reserved_per_block, int32_t regs_blocks_per_sm,
+                  tmc_plan *out, tmc_status *st) {
+    set_status(st, TMC_OK, "");
+    if (!spec || !opt || !out || sms < 1 || smem_per_sm < 1024 || smem_per_block_optin < 1024 ||
+        reserved_per_block < 0) {
+        set_status(st, TMC_BAD_ARGUMENT, "NULL argument or impossible device limits");
+        return TMC_BAD_ARGUMENT;
+    }
+    try {
+        validate_run(*spec, *opt);
+        const DeviceLimits lim{sms, static_cast<size_t>(smem_per_sm), static_cast<size_t>(smem_per_block_optin),
+                               static_cast<size_t>(reserved_per_block)};
+        const Plan p = make_plan(*spec, *opt, lim, regs_blocks_per_sm);
+        const WalkParams P = make_params(*spec, *opt, p, nullptr, nullptr);
+        out->threads = p.threads;
+        out->blocks_per_sm = p.blocks_per_sm;
+        out->grid = p.grid;
+        out->tr_a = p.tr_a;
+        out->tz_a = p.tz_a;
+        out->cross = p.cross;
+        out->tr_rd = p.tr_rd;
+        out->tr_tt = p.tr_tt;
+        out->batch_smem = p.batch_smem;
+        out->smem_bytes = static_cast<int32_t>(plan_smem_bytes(P));
+        return TMC_OK;
+    } catch (const ConfigFailure &e) {
+        set_status(st, TMC_BAD_CONFIG, e.what());
+        return TMC_BAD_CONFIG;
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,150 @@
+// Device side of the B200 photon walk: the per-lane state machine and one MCML step.
+//
+// Step semantics follow TissueMC's include/tissuemc/physics.hpp (launch :58-66, Fresnel :71-98,
+// Henyey-Greenstein :101-113, spin :116-144, step size :148-158, boundary :162-178, hop :180-184,
+// drop :187-193, crossing :198-246, roulette :250-259, step_once :263-277) and its Philox stream
+// (include/tissuemc/philox.hpp:49-57, 91-122, 133-136), so photon i sees the same random words as
+// on the CPU. The structure is this engine's own:
+//
+//  * a lane is one thread of a persistent, warp-synchronous loop; a lane whose photon ends claims
+//    the next id from a per-warp pool, which the warp refills from a global counter in chunks;
+//  * all photon state, the random stream (a 6-word queue refilled once per step) and the hot
+//    constants of the current layer live in registers; the layer table lives in shared memory and
+//    is read only when a packet changes layer or meets a boundary;
+//  * every tally is an unsigned 64-bit fixed-point integer (weight * 2^32, rounded), so sums are
+//    exact and a run's output does not depend on scheduling; per-photon values (events, absorbed
+//    weight in the current layer, the exit weight) accumulate in registers and are published once
+//    per photon (or per layer change) into per-block shared-memory batch totals.
+#pragma once
+
+#include <cstdint>
+
+namespace tmc {
+
+constexpr int kMaxLayers = 16;
+constexpr float kFixedScale = 4294967296.0f;  // 2^32
+
+// Constants of one layer, computed on the host in float arithmetic in the same order as the
+// reference evaluates them (so e.g. hg_a is exactly float(1) - g * g).
+struct LayerC {
+    float mua, mus, mut, inv_mut;     // mut = mua + mus
+    float absorb;                     // mua / mut
+    float z0, z1;                     // top and bottom depth [cm]
+    float g, hg_a, hg_b, hg_c, hg_d;  // 1 - g*g, 1 - g, 2*g, 1 + g*g
+    float inv_2g;                     // 1 / (2*g), 0 when g == 0
+    float n, n_up, n_dn;              // this layer's index and its neighbours' (ambient at the ends)
+    float cc_up, cc_dn;               // critical cosines toward the top and the bottom (0 if none)
+    float rat_up, rat_dn;             // n / n_up, n / n_dn
+    float rn_up, rn_dn;               // normal-incidence Fresnel reflectance toward each side
+    float pad[2];
+};
+static_assert(sizeof(LayerC) == 24 * 4, "LayerC layout");
+
+// Everything the walk kernel needs, passed by value (__grid_constant__).
+struct WalkParams {
+    uint64_t photons;      // photon ids [0, photons)
+    uint64_t seed;         // Philox key
+    uint64_t plan_base;    // BatchPlan: photons per batch before the remainder
+    uint64_t plan_extra;   // BatchPlan: the first `extra` batches hold one more
+    unsigned long long *counter;   // next unclaimed photon id (zeroed before launch)
+    unsigned long long *g_batch;   // [nb * (4 + nl)] rd, tt, events, anomalies, absorbed[nl]
+    unsigned long long *g_arz;     // [nr * nz]
+    unsigned long long *g_rd;      // [nr * na]
+    unsigned long long *g_tt;      // [nr * na]
+    int nb, nl, nz, nr, na;
+    float launch_w;        // 1 - specular reflectance, in float as the reference's launch()
+    float dz, dr, da;      // bin widths (da = pi / (2 na))
+    float inv_dz, inv_dr, inv_da;
+    int tr_a, tz_a;        // shared tile of A(r,z): ir < tr_a and iz < tz_a
+    int tr_rd, tr_tt;      // shared tiles of R_d(r,a) and T_t(r,a): ir < tr (all angles)
+    int cross;             // 1: the clamped last row and column of A(r,z) are in shared memory too
+    int batch_smem;        // 1: per-batch totals in shared memory
+    int profiles;          // 0: skip A(r,z), R_d(r,a), T_t(r,a)
+    uint32_t step_cap;     // a packet still alive after this many steps is ended as an anomaly
+    int chunk;             // photon ids claimed per warp refill (>= 32)
+    LayerC layers[kMaxLayers];
+};
+
+// ------------------------------------------------------------------------------------ Philox
+__device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t k0,
+                                              uint32_t k1, uint32_t &o0, uint32_t &o1,
+                                              uint32_t &o2, uint32_t &o3) {
+    uint32_t c3 = 0u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * c0;
+        const uint64_t p1 = static_cast<uint64_t>(0xCD9E8D57u) * c2;
+        const uint32_t n0 = static_cast<uint32_t>(p1 >> 32) ^ c1 ^ k0;
+        const uint32_t n2 = static_cast<uint32_t>(p0 >> 32) ^ c3 ^ k1;
+        c0 = n0;
+        c1 = static_cast<uint32_t>(p1);
+        c2 = n2;
+        c3 = static_cast<uint32_t>(p0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    o0 = c0;
+    o1 = c1;
+    o2 = c2;
+    o3 = c3;
+}
+
+// Uniform on (0,1) from one word, keeping 23 bits (philox.hpp:133-136).
+__device__ __forceinline__ float unit_open(uint32_t x) {
+    return (static_cast<float>(x >> 9) + 0.5f) * 0x1p-23f;
+}
+
+// ------------------------------------------------------------------------------------ math
+// The walk is compiled in two variants: exact (MODE 0: IEEE division and square root, the
+// accurate logf/sincosf, the reference's operation order) and fast (MODE 1). What "fast" replaces
+// is the bit mask TMC_FAST_MASK, chosen so that the fast variant still meets the reference's
+// identical-photon limits against the float32 CPU engine:
+//   1: __logf for the step length          2: __sincosf for the azimuth
+//   4: SFU reciprocal division and precomputed reciprocals (1/mu_t, mu_a/mu_t, 1/(2g), 10 for 1/0.1)
+//   8: sqrt.approx and rsqrt (renormalisation, Fresnel, radius)
+#ifndef TMC_FAST_MASK
+#define TMC_FAST_MASK 15
+#endif
+
+template <int MODE> struct Math {
+    static constexpr int mask = MODE ? TMC_FAST_MASK : 0;
+    static constexpr bool log = (mask & 1) != 0;
+    static constexpr bool sincos = (mask & 2) != 0;
+    static constexpr bool div = (mask & 4) != 0;
+    static constexpr bool sqrt = (mask & 8) != 0;
+};
+
+template <int MODE> __device__ __forceinline__ float m_div(float a, float b) {
+    if constexpr (Math<MODE>::div) return __fdividef(a, b);
+    else return a / b;
+}
+template <int MODE> __device__ __forceinline__ float m_sqrt(float x) {
+    if constexpr (Math<MODE>::sqrt) {
+        float r;
+        asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+        return r;
+    } else {
+        return sqrtf(x);
+    }
+}
+template <int MODE> __device__ __forceinline__ float m_rsqrt(float x) {
+    if constexpr (Math<MODE>::sqrt) return rsqrtf(x);
+    else return 1.0f / sqrtf(x);
+}
+template <int MODE> __device__ __forceinline__ float m_log(float x) {
+    if constexpr (Math<MODE>::log) return __logf(x);
+    else return logf(x);
+}
+
+__device__ __forceinline__ unsigned long long to_fixed(float w) {
+    return __float2ull_rn(w * kFixedScale);
+}
+
+// Clamped bin index (src/cpu/engine.cpp:59-66): non-positive (or NaN) -> 0, beyond -> last.
+__device__ __forceinline__ int clamp_bin(float x, float inv_width, int count) {
+    if (!(x > 0.0f)) return 0;
+    const float i = x * inv_width;
+    return i >= static_cast<float>(count) ? count - 1 : static_cast<int>(i);
+}
+
+}  // namespace tmc
