@@ -174,6 +174,30 @@ TMC_B200_API int tmc_b200_plan(const tmc_run_spec *spec, const tmc_options *opt,
                   int64_t smem_per_block_optin, int64_t reserved_per_block, int32_t regs_blocks_per_sm,
                   tmc_plan *plan, tmc_status *status);
 
+/* Capacity of the static scratch used by tmc_b200_run_static, in 64-bit tally words (512 KiB). */
+#define TMC_B200_STATIC_SCRATCH_WORDS 65536u
+
+/* Run the walk without allocating anything. No counterpart in the reference: it exists for callers
+ * that cannot call cudaMalloc, such as a host program that runs while a stream is being captured
+ * into a CUDA graph (allocation is not permitted then) or a framework that owns all device memory
+ * through its own pool. Results are as tmc_b200_run's, bit for bit.
+ *
+ * The walk's scratch (its photon-claim counter and the fixed-point tally accumulators) lives in a
+ * static device array of the library, TMC_B200_STATIC_SCRATCH_WORDS words plus a 256-byte head,
+ * which every GPU that loads the library holds until the process exits. Runs whose tally buffer
+ * (tmc_sizes.tally_words) is larger are rejected with TMC_BAD_CONFIG. The caller passes every
+ * output, including result->raw (tally_words host words), which receives the fixed-point tallies
+ * and is then decoded into the other arrays. No cudaMalloc, cudaFree, stream or event creation,
+ * and no host-side allocation on success.
+ *
+ * The first call on a device sets up that device (the array's device address, the kernels'
+ * shared-memory limit); make it before any stream capture begins. Each call clears the parts of
+ * the array it uses and runs on the legacy default stream, synchronously. Every call shares the
+ * one array: calls serialise on the host, and calls that could overlap on the GPU (from other
+ * code paths on other streams) would race. kernel_seconds is measured by the host clock here. */
+TMC_B200_API int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_result *result,
+                                     tmc_status *status);
+
 /* Parse an MCML .mci file (the reference's parse_mci_file, src/io/mci.cpp:173-183): writes up to
  * `max_runs` runs and returns the number found in *n_runs. Errors carry the line number. */
 TMC_B200_API int tmc_b200_parse_mci(const char *path, tmc_run_spec *runs, int32_t max_runs, int32_t *n_runs,

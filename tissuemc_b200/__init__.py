@@ -120,6 +120,7 @@ PROTOTYPES = {
     "tmc_b200_decode": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _pu, _P(CResult), _P(CStatus)]),
     "tmc_b200_parse_mci": (ctypes.c_int, [ctypes.c_char_p, _P(CRunSpec), ctypes.c_int32,
                                           _P(ctypes.c_int32), _P(CStatus)]),
+    "tmc_b200_run_static": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _P(CResult), _P(CStatus)]),
     "tmc_b200_plan": (ctypes.c_int, [_P(CRunSpec), _P(COptions), ctypes.c_int32, ctypes.c_int64,
                                      ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _P(CPlan),
                                      _P(CStatus)]),
@@ -331,6 +332,24 @@ def run(spec: RunSpec, opt: COptions | None = None, **kw) -> RunResult:
     st = CStatus()
     c = spec.to_c()
     _check(lib().tmc_b200_run(ctypes.byref(c), ctypes.byref(opt), ctypes.byref(res), ctypes.byref(st)), st)
+    return RunResult(spec=spec, seed=opt.seed, specular=res.specular, kernel_seconds=res.kernel_seconds,
+                     wall_seconds=res.wall_seconds, device=res.device.decode(), rung=opt.rung,
+                     profiles=bool(opt.profiles), **arrs)
+
+
+STATIC_SCRATCH_WORDS = 65536
+
+
+def run_static(spec: RunSpec, opt: COptions | None = None, **kw) -> RunResult:
+    """Run the walk through the allocation-free entry point (tmc_b200_run_static): the library
+    allocates nothing; its scratch is a static device array of STATIC_SCRATCH_WORDS tally words."""
+    if opt is None:
+        opt = options(**kw)
+    sz = query_sizes(spec, opt)
+    arrs, res = _alloc_result(sz)
+    st = CStatus()
+    c = spec.to_c()
+    _check(lib().tmc_b200_run_static(ctypes.byref(c), ctypes.byref(opt), ctypes.byref(res), ctypes.byref(st)), st)
     return RunResult(spec=spec, seed=opt.seed, specular=res.specular, kernel_seconds=res.kernel_seconds,
                      wall_seconds=res.wall_seconds, device=res.device.decode(), rung=opt.rung,
                      profiles=bool(opt.profiles), **arrs)

@@ -279,6 +279,52 @@ void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
 }
 
 }  // namespace
+// ------------------------------------------------------------- allocation-free entry point
+// Some callers cannot allocate device memory: a host program that runs while a CUDA stream is
+// being captured into a graph (cudaMalloc is not permitted during capture), or a framework that
+// owns every byte of device memory through its own pool and forbids libraries from calling
+// cudaMalloc. tmc_b200_run_static serves them: the walk's scratch (its photon-claim counter and
+// the fixed-point tally accumulators) lives in the file-scope array below, which the CUDA
+// runtime places in every device's memory when the library is loaded and keeps until exit.
+namespace {
+
+constexpr size_t kStaticHeadWords = 32;  // word 0: claim counter; the tallies start 256 B in
+__device__ __align__(256) unsigned long long g_static_scratch[kStaticHeadWords + TMC_B200_STATIC_SCRATCH_WORDS];
+
+struct StaticDevice {
+    bool ready = false;
+    cudaDeviceProp prop{};
+    unsigned long long *scratch = nullptr;  // device address of g_static_scratch on this device
+};
+StaticDevice g_static_dev[kMaxDevices];
+
+// Once per device, with that device current: the array's device address (its name in host code
+// is only a host-side stand-in) and the kernels' shared-memory limit.
+StaticDevice &static_device(int dev) {
+    if (dev < 0 || dev >= kMaxDevices) throw Fail(TMC_BAD_CONFIG, "device ordinal out of range");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0 || dev >= n) {
+        cudaGetLastError();
+        throw Fail(TMC_NO_DEVICE, "no usable CUDA device found");
+    }
+    TMC_CUDA(cudaSetDevice(dev));
+    StaticDevice &d = g_static_dev[dev];
+    if (!d.ready) {
+        TMC_CUDA(cudaGetDeviceProperties(&d.prop, dev));
+        void *addr = nullptr;
+        TMC_CUDA(cudaGetSymbolAddress(&addr, g_static_scratch));
+        d.scratch = static_cast<unsigned long long *>(addr);
+        TMC_CUDA(cudaFuncSetAttribute(walk_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      d.prop.sharedMemPerBlockOptin));
+        TMC_CUDA(cudaFuncSetAttribute(walk_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      d.prop.sharedMemPerBlockOptin));
+        d.ready = true;
+    }
+    return d;
+}
+
+}  // namespace
+
 }  // namespace tmc
 
 // ================================================================================== C ABI
@@ -349,6 +395,71 @@ int tmc_b200_run_device(const tmc_run_spec *spec, const tmc_options *opt, uint64
         DeviceCtx &c = device_ctx(opt->device);
         launch_walk(*spec, *opt, c, reinterpret_cast<unsigned long long *>(d_tally),
                     static_cast<cudaStream_t>(stream), nullptr, nullptr);
+        return TMC_OK;
+    } catch (const ConfigFailure &e) {
+        set_status(st, TMC_BAD_CONFIG, e.what());
+        return TMC_BAD_CONFIG;
+    } catch (const Fail &e) {
+        set_status(st, e.code(), e.what());
+        return e.code();
+    } catch (const std::exception &e) {
+        set_status(st, TMC_CUDA_ERROR, e.what());
+        return TMC_CUDA_ERROR;
+    }
+}
+
+int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_result *res, tmc_status *st) {
+    set_status(st, TMC_OK, "");
+    if (!spec || !opt || !res || !res->raw) {
+        set_status(st, TMC_BAD_ARGUMENT, "NULL argument (tmc_b200_run_static needs result->raw as well)");
+        return TMC_BAD_ARGUMENT;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    std::lock_guard<std::mutex> lock(g_mu);
+    try {
+        validate_run(*spec, *opt);
+        const RunShape sh = shape_of(*spec, *opt);
+        const size_t words = tally_offsets(sh).total;
+        if (words > TMC_B200_STATIC_SCRATCH_WORDS) {
+            throw Fail(TMC_BAD_CONFIG,
+                       "this run needs " + std::to_string(words) + " tally words but the static scratch of "
+                       "tmc_b200_run_static holds " + std::to_string(TMC_B200_STATIC_SCRATCH_WORDS) +
+                       " (fewer batches or bins, or use tmc_b200_run)");
+        }
+        StaticDevice &d = static_device(opt->device);
+        unsigned long long *counter = d.scratch;
+        unsigned long long *tally = d.scratch + kStaticHeadWords;
+        int regs_bps = 0;
+        const int threads = opt->threads_per_block > 0 ? opt->threads_per_block : 256;
+        if (opt->fast_math)
+            TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&regs_bps, walk_kernel<1>, threads, 0));
+        else
+            TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&regs_bps, walk_kernel<0>, threads, 0));
+        const Plan pl = make_plan(*spec, *opt, limits_of(d.prop), regs_bps);
+        WalkParams P = make_params(*spec, *opt, pl, tally, counter);
+        const size_t smem = plan_smem_bytes(P);
+        if (smem > d.prop.sharedMemPerBlockOptin)
+            throw Fail(TMC_BAD_CONFIG, "the tally plan does not fit in shared memory");
+        const uint64_t max_blocks = (sh.photons + pl.threads - 1) / pl.threads;
+        const int grid = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(pl.grid), max_blocks));
+        // the array keeps the previous call's contents: the counter and the tallies start at zero
+        TMC_CUDA(cudaMemsetAsync(d.scratch, 0, (kStaticHeadWords + words) * 8, 0));
+        const auto k0 = std::chrono::steady_clock::now();
+        if (opt->fast_math)
+            walk_kernel<1><<<grid, pl.threads, smem, 0>>>(P);
+        else
+            walk_kernel<0><<<grid, pl.threads, smem, 0>>>(P);
+        TMC_CUDA(cudaGetLastError());
+        TMC_CUDA(cudaMemcpy(res->raw, tally, words * 8, cudaMemcpyDeviceToHost));
+        const auto k1 = std::chrono::steady_clock::now();
+        uint64_t *raw = res->raw;
+        res->raw = nullptr;  // decode into the other arrays without copying raw onto itself
+        decode_tallies(*spec, *opt, raw, *res);
+        res->raw = raw;
+        res->kernel_seconds = std::chrono::duration<double>(k1 - k0).count();
+        std::snprintf(res->device, sizeof res->device, "%.100s (sm_%d%d)", d.prop.name, d.prop.major,
+                      d.prop.minor);
+        res->wall_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         return TMC_OK;
     } catch (const ConfigFailure &e) {
         set_status(st, TMC_BAD_CONFIG, e.what());
