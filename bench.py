@@ -31,9 +31,13 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+SWEEP_DESC = ("4096 configurations drawn by tmc_b200_sweep_sample(master seed 1): 1-3 layers, "
+              "mua logU[0.01,10], mus' logU[1,50], g U[0.7,0.95], n U[1.33,1.5], d logU[0.01,1] cm, "
+              "photons logU[1e4,1e6] (9.07e8 in all); grid nr=nz=64, dr=dz=0.01 cm, na=1; 10 batches each")
 WORKLOADS = {
     "skin5": "five-layer skin stack (n=1.4 in air; 1e8 photons; dr=0.002 cm x 500, dz=0.001 cm x 400, na=30)",
     "slab_n14": "single slab n=1.4 in air (mua=5, mus=95, g=0.8, d=0.05 cm; 1e6 photons; 50x20 grid, na=30)",
+    "sweep": SWEEP_DESC,
 }
 METRIC = "photons/s on 1 B200 (plain MC)"
 
@@ -58,6 +62,9 @@ def _args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--photons", type=int, default=0,
                     help="override the workload's photon count (for profiling captures only)")
+    ap.add_argument("--autotune", action="store_true", help="sweep: pick the launch shape first")
+    ap.add_argument("--no-profiles", action="store_true",
+                    help="diagnostic: skip the profile tallies (rung 6 without profiles); not a result")
     return ap.parse_args()
 
 
@@ -184,10 +191,56 @@ def run_reference_arm(a) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_sweep(a) -> None:
+    """Batched sweep: solves/s of the graph-captured persistent launch, beside the loop of
+    single-run launches over the same configurations (equal total photons)."""
+    import time
+
+    import tissuemc_b200 as tmc
+
+    rank, world, local = _dist()
+    cfgs = tmc.sweep_sample(1 + rank, 4096)
+    opt = tmc.sweep_options(device=local)
+    if a.autotune:
+        opt, _ = tmc.sweep_autotune(cfgs, opt)
+    for _ in range(a.warmup):
+        tmc.sweep_run(cfgs, opt)
+    with Clocks(local) as clk:
+        kern, wall = [], []
+        for _ in range(a.steps):
+            t0 = time.perf_counter()
+            r = tmc.sweep_run(cfgs, opt)
+            wall.append(time.perf_counter() - t0)
+            kern.append(r.seconds)
+    loop = tmc.sweep_run_loop(cfgs, opt).seconds
+    n = len(cfgs)
+    ks, ws = sum(kern) / len(kern), sum(wall) / len(wall)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "solves/s on 1 B200 (batched sweep)", "value": world * n / ks, "unit": "solves/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * ks,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 transport, u64 fixed-point tallies", "data": "synthetic (seeded configurations)",
+            "config": {"workload": f"sweep: {SWEEP_DESC}", "threads_per_block": opt.threads_per_block,
+                       "item_photons": opt.item_photons, "autotuned": bool(a.autotune)},
+            "e2e": {"value": world * n / ws, "unit": "solves/s",
+                    "h2d_bytes_per_step": n * 48 + n * 4 + sum(c.num_layers for c in cfgs) * 96,
+                    "d2h_bytes_per_step": n * (opt.nr + 3) * 8},
+            "loop_baseline": {"value": n / loop, "unit": "solves/s", "seconds": loop,
+                              "what": "one single-run walk launch per configuration, back to back on one stream"},
+            "speedup_vs_loop": loop / ks,
+            "photons_per_s": sum(int(c.photons) for c in cfgs) / ks,
+            "gpu_launches": a.steps * 2, "clocks": clk.summary(),
+        }), flush=True)
+
+
 def main() -> None:
     a = _args()
     if a.impl == "reference":
         run_reference_arm(a)
+        return
+    if a.workload == "sweep":
+        run_sweep(a)
         return
     import ctypes
 
@@ -208,7 +261,8 @@ def main() -> None:
     if a.photons:
         spec.photons = a.photons
     photons = spec.photons
-    opt = tmc.options(batches=a.batches, seed=1 + 1000003 * rank, device=local)
+    opt = tmc.options(batches=a.batches, seed=1 + 1000003 * rank, device=local,
+                      rung=6 if a.no_profiles else 0, profiles=not a.no_profiles)
     words = int(tmc.query_sizes(spec, opt).tally_words)
     d_tally = torch.empty(words, dtype=torch.int64, device=f"cuda:{local}")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
@@ -284,6 +338,7 @@ def main() -> None:
             "data": "synthetic (the workload's .mci; seeded Philox photons)",
             "config": {"workload": f"{a.workload}: {WORKLOADS[a.workload]}", "photons_per_step": photons,
                        "batches": a.batches, "l2": "flushed between steps (256 MB write)",
+                       "profiles": not a.no_profiles,
                        "parallelism": "replicas" if world > 1 else "1 GPU"},
             "e2e": e2e,
             "gpu_launches": a.steps,

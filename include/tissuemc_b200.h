@@ -198,6 +198,71 @@ TMC_B200_API int tmc_b200_plan(const tmc_run_spec *spec, const tmc_options *opt,
 TMC_B200_API int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_result *result,
                                      tmc_status *status);
 
+/* ------------------------------------------------------------------ batched sweep
+ * Thousands of independent tissue configurations in one persistent, CUDA-graph-captured launch.
+ * No counterpart in the reference (an addition of this engine). Every configuration shares the
+ * grid and batch count of the options; each runs its own photons with its own Philox seed, and
+ * its tallies are bit for bit those of tmc_b200_run on that configuration alone (same seed,
+ * photons, batches, grid and math). */
+typedef struct {
+    uint64_t photons;          /* >= batches */
+    uint64_t seed;             /* Philox key of this configuration's photon streams */
+    double n_above, n_below;   /* ambient refractive indices */
+    int32_t num_layers;
+    tmc_layer layers[TMC_B200_MAX_LAYERS];
+} tmc_sweep_config;
+
+typedef struct {
+    double dz, dr;             /* grid shared by every configuration */
+    int32_t nz, nr, na;
+    int32_t batches;           /* per configuration */
+    int32_t fast_math;         /* as tmc_options */
+    int32_t profiles;          /* 0: totals only */
+    int32_t device;
+    int32_t threads_per_block; /* 0 = 256 */
+    int32_t item_photons;      /* photons per work-queue item; 0 = 256 */
+} tmc_sweep_options;
+
+typedef struct {
+    uint64_t words_per_config;   /* raw tally words per configuration: the single-run layout with
+                                    max_layers layer slots in every batch row */
+    uint64_t summary_per_config; /* nr + 3: R_d(r) per photon, then R_d, T_t, A per photon */
+    int32_t max_layers;
+} tmc_sweep_sizes;
+
+/* Options for the sweep workload of this engine's benchmark: grid nr = nz = 64, dr = dz = 0.01 cm,
+ * na = 1, 10 batches, fast math, 256 threads, 256 photons per item. */
+TMC_B200_API void tmc_b200_sweep_default_options(tmc_sweep_options *opt);
+
+/* Draw n configurations: 1-3 layers sharing one refractive index n ~ U[1.33, 1.5] in air;
+ * per layer mua ~ logU[0.01, 10] /cm, reduced scattering mus' ~ logU[1, 50] /cm, g ~ U[0.7, 0.95]
+ * (mus = mus' / (1 - g)), thickness ~ logU[0.01, 1] cm; photons ~ logU[1e4, 1e6]; a 64-bit seed
+ * per configuration. Draws come from Philox keyed by master_seed with the configuration index in
+ * the counter, so configuration c does not depend on n. */
+TMC_B200_API int tmc_b200_sweep_sample(uint64_t master_seed, int32_t n, tmc_sweep_config *out, tmc_status *status);
+
+/* Validate every configuration (messages name the configuration) and report buffer sizes. */
+TMC_B200_API int tmc_b200_sweep_sizes(const tmc_sweep_config *cfgs, int32_t n, const tmc_sweep_options *opt,
+                                      tmc_sweep_sizes *sizes, tmc_status *status);
+
+/* Run the sweep: one captured graph (table upload, zeroing, the persistent sweep kernel, the
+ * per-configuration summary kernel, summary download), cached per device and reused while the
+ * shape allows. raw (optional, host): n * words_per_config words; summary (optional, host):
+ * n * summary_per_config doubles; kernel_seconds (optional): device time of the sweep kernel. */
+TMC_B200_API int tmc_b200_sweep_run(const tmc_sweep_config *cfgs, int32_t n, const tmc_sweep_options *opt,
+                                    uint64_t *raw, double *summary, double *kernel_seconds, tmc_status *status);
+
+/* The baseline the sweep replaces: the same configurations as a loop of single-run launches of
+ * the walk kernel on one stream (one launch per configuration). raw (optional) as above;
+ * seconds: device time from the first launch to the end of the last. */
+TMC_B200_API int tmc_b200_sweep_run_loop(const tmc_sweep_config *cfgs, int32_t n, const tmc_sweep_options *opt,
+                                         uint64_t *raw, double *seconds, tmc_status *status);
+
+/* Autotune the sweep's launch shape on these configurations: block size {128, 256} x photons per
+ * work item {64, 256, 1024}, each timed on a second run; writes the fastest into *opt. */
+TMC_B200_API int tmc_b200_sweep_autotune(const tmc_sweep_config *cfgs, int32_t n, tmc_sweep_options *opt,
+                                         double *best_seconds, tmc_status *status);
+
 /* Parse an MCML .mci file (the reference's parse_mci_file, src/io/mci.cpp:173-183): writes up to
  * `max_runs` runs and returns the number found in *n_runs. Errors carry the line number. */
 TMC_B200_API int tmc_b200_parse_mci(const char *path, tmc_run_spec *runs, int32_t max_runs, int32_t *n_runs,

@@ -1,0 +1,172 @@
+"""The batched sweep: the configuration sampler and validation (CPU), and on the GPU bit-for-bit
+agreement of every configuration with its own single run, graph reuse across sweeps, the plain
+loop baseline, the autotuner, the per-configuration summaries, and oracle parity on a few
+configurations."""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+import tissuemc_b200 as tmc
+from gates import from_engine, from_oracle, identical_photon_gaps
+
+
+def _scaled(cfgs, cap):
+    """A copy of the configurations with photon counts capped (tests need small runs)."""
+    out = (tmc.CSweepConfig * len(cfgs))()
+    for i, c in enumerate(cfgs):
+        out[i] = c
+        out[i].photons = min(int(c.photons), cap)
+    return out
+
+
+def test_sampler_is_deterministic_and_in_range():
+    a = tmc.sweep_sample(11, 512)
+    b = tmc.sweep_sample(11, 40)
+    assert all(bytes(a[i]) == bytes(b[i]) for i in range(40))  # config c does not depend on n
+    assert bytes(tmc.sweep_sample(12, 1)[0]) != bytes(a[0])
+    for c in a:
+        assert 1 <= c.num_layers <= 3 and 10_000 <= c.photons <= 1_000_000
+        assert c.n_above == 1.0 and c.n_below == 1.0
+        ns = {c.layers[i].n for i in range(c.num_layers)}
+        assert len(ns) == 1 and 1.33 <= ns.pop() <= 1.5
+        for i in range(c.num_layers):
+            L = c.layers[i]
+            assert 0.01 <= L.mua <= 10 and 0.7 <= L.g <= 0.95 and 0.01 <= L.d <= 1
+            assert 1 <= L.mus * (1 - L.g) <= 50 * (1 + 1e-12)
+    counts = np.bincount([c.num_layers for c in a], minlength=4)[1:]
+    assert counts.min() > 120  # about a third each
+
+
+def test_sizes_and_validation_name_the_configuration():
+    cfgs = tmc.sweep_sample(3, 8)
+    opt = tmc.sweep_options()
+    sz = tmc.sweep_sizes(cfgs, opt)
+    lmax = max(c.num_layers for c in cfgs)
+    assert sz.max_layers == lmax
+    assert sz.words_per_config == 10 * (4 + lmax) + 64 * 64 + 2 * 64
+    assert sz.summary_per_config == 67
+    cfgs[5].layers[0].g = 1.0
+    with pytest.raises(tmc.ConfigError, match="configuration 5: layer 1: g must be in"):
+        tmc.sweep_sizes(cfgs, opt)
+    cfgs = tmc.sweep_sample(3, 2)
+    cfgs[1].photons = 3
+    with pytest.raises(tmc.ConfigError, match="configuration 1: batches cannot exceed"):
+        tmc.sweep_sizes(cfgs, opt)
+    with pytest.raises(tmc.ConfigError, match="item_photons"):
+        tmc.sweep_sizes(tmc.sweep_sample(3, 2), tmc.sweep_options(item_photons=-1))
+
+
+def _single_run_raw(c, opt):
+    """One configuration through tmc_b200_run, widened to the sweep layout."""
+    spec = tmc.config_spec(c, opt)
+    r = tmc.run(spec, photons=int(c.photons), batches=opt.batches, seed=int(c.seed), fast_math=bool(opt.fast_math))
+    return r
+
+
+@pytest.mark.gpu
+def test_every_configuration_equals_its_single_run_bit_for_bit():
+    opt = tmc.sweep_options()
+    cfgs = _scaled(tmc.sweep_sample(21, 48), 6000)
+    res = tmc.sweep_run(cfgs, opt, raw=True)
+    lmax = max(c.num_layers for c in cfgs)
+    nb = opt.batches
+    for i, c in enumerate(cfgs):
+        r = _single_run_raw(c, opt)
+        nl = c.num_layers
+        block = res.raw[i]
+        rows = block[: nb * (4 + lmax)].reshape(nb, 4 + lmax)
+        assert np.array_equal(rows[:, : 4 + nl], r.raw[: nb * (4 + nl)].reshape(nb, 4 + nl)), i
+        assert not rows[:, 4 + nl:].any()
+        assert np.array_equal(block[nb * (4 + lmax):], r.raw[nb * (4 + nl):]), i
+
+
+@pytest.mark.gpu
+def test_loop_baseline_gives_the_same_tallies():
+    opt = tmc.sweep_options()
+    cfgs = _scaled(tmc.sweep_sample(5, 64), 4000)
+    a = tmc.sweep_run(cfgs, opt, raw=True)
+    b = tmc.sweep_run_loop(cfgs, opt, raw=True)
+    assert np.array_equal(a.raw, b.raw)
+    assert a.seconds > 0 and b.seconds > 0
+
+
+@pytest.mark.gpu
+def test_graph_is_reused_for_new_configurations_and_stays_exact():
+    opt = tmc.sweep_options()
+    first = _scaled(tmc.sweep_sample(100, 96), 3000)
+    second = _scaled(tmc.sweep_sample(200, 40), 5000)  # fewer configurations: same captured graph
+    a1 = tmc.sweep_run(first, opt, raw=True)
+    b = tmc.sweep_run(second, opt, raw=True)
+    a2 = tmc.sweep_run(first, opt, raw=True)
+    assert np.array_equal(a1.raw, a2.raw) and np.array_equal(a1.summary, a2.summary)
+    ref = tmc.sweep_run_loop(second, opt, raw=True)
+    assert np.array_equal(b.raw, ref.raw)
+
+
+@pytest.mark.gpu
+def test_summaries_follow_from_the_tallies():
+    opt = tmc.sweep_options()
+    cfgs = _scaled(tmc.sweep_sample(9, 32), 8000)
+    res = tmc.sweep_run(cfgs, opt, raw=True)
+    nb, nr = opt.batches, opt.nr
+    for i, c in enumerate(cfgs):
+        lmax = (res.raw.shape[1] - nr * opt.nz - 2 * nr * opt.na) // nb - 4
+        rows = res.raw[i, : nb * (4 + lmax)].reshape(nb, 4 + lmax).astype(np.float64)
+        k = 1.0 / (2.0**32 * int(c.photons))
+        s = res.summary[i]
+        assert math.isclose(s[nr], rows[:, 0].sum() * k, rel_tol=1e-12)
+        assert math.isclose(s[nr + 1], rows[:, 1].sum() * k, rel_tol=1e-12, abs_tol=1e-300)
+        assert math.isclose(s[nr + 2], rows[:, 4:].sum() * k, rel_tol=1e-12)
+        assert math.isclose(s[:nr].sum(), s[nr], rel_tol=1e-9)
+        spec = tmc.config_spec(c, opt)
+        rsp = ((spec.n_above - spec.layers[0][0]) / (spec.n_above + spec.layers[0][0])) ** 2
+        assert abs(s[nr] + s[nr + 1] + s[nr + 2] + rsp - 1) < 5e-3  # conservation per configuration
+
+
+@pytest.mark.gpu
+def test_autotuner_picks_a_valid_shape():
+    cfgs = _scaled(tmc.sweep_sample(8, 128), 2000)
+    opt, best = tmc.sweep_autotune(cfgs, tmc.sweep_options())
+    assert opt.threads_per_block in (128, 256) and opt.item_photons in (64, 256, 1024)
+    assert best > 0
+    ref = tmc.sweep_run(cfgs, tmc.sweep_options(), raw=True)
+    tuned = tmc.sweep_run(cfgs, opt, raw=True)
+    assert np.array_equal(ref.raw, tuned.raw)  # the launch shape never changes results
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("idx", [0, 1, 2])
+def test_sweep_configurations_match_the_oracle_on_identical_photons(idx):
+    opt = tmc.sweep_options()
+    cfgs = _scaled(tmc.sweep_sample(77, 3), 200_000)
+    res = tmc.sweep_run(cfgs, opt, raw=True)
+    c = cfgs[idx]
+    spec = tmc.config_spec(c, opt)
+    g = tmc.decode(spec, tmc.options(photons=int(c.photons), batches=opt.batches, seed=int(c.seed)),
+                   _narrow(res.raw[idx], max(x.num_layers for x in cfgs), c.num_layers, opt))
+    o = oracle.run(oracle.Spec(layers=list(spec.layers), dz=spec.dz, dr=spec.dr, nz=spec.nz, nr=spec.nr,
+                               na=spec.na, n_above=spec.n_above, n_below=spec.n_below),
+                   int(c.photons), opt.batches, int(c.seed), 32, threads=0)
+    bad = [str(x) for x in identical_photon_gaps(from_oracle(o), from_engine(g)) if not x.passed]
+    assert not bad, bad
+
+
+def _narrow(block, lmax, nl, opt):
+    nb = opt.batches
+    rows = block[: nb * (4 + lmax)].reshape(nb, 4 + lmax)[:, : 4 + nl].ravel()
+    return np.concatenate([rows, block[nb * (4 + lmax):]])
+
+
+@pytest.mark.gpu
+def test_single_configuration_and_sixteen_layers():
+    opt = tmc.sweep_options(batches=4)
+    spec = tmc.RunSpec(layers=[(1.3 + 0.01 * i, 0.5, 20 + i, 0.8, 0.02) for i in range(16)])
+    cfgs = (tmc.CSweepConfig * 1)(tmc.sweep_config(spec, 20_000, 99))
+    res = tmc.sweep_run(cfgs, opt, raw=True)
+    r = _single_run_raw(cfgs[0], opt)
+    assert np.array_equal(res.raw[0], r.raw)

@@ -106,6 +106,28 @@ class CPlan(ctypes.Structure):
                  "batch_smem", "smem_bytes")]
 
 
+class CSweepConfig(ctypes.Structure):
+    _fields_ = [
+        ("photons", ctypes.c_uint64),
+        ("seed", ctypes.c_uint64),
+        ("n_above", ctypes.c_double),
+        ("n_below", ctypes.c_double),
+        ("num_layers", ctypes.c_int32),
+        ("layers", Layer * MAX_LAYERS),
+    ]
+
+
+class CSweepOptions(ctypes.Structure):
+    _fields_ = [("dz", ctypes.c_double), ("dr", ctypes.c_double)] + [
+        (k, ctypes.c_int32) for k in ("nz", "nr", "na", "batches", "fast_math", "profiles", "device",
+                                      "threads_per_block", "item_photons")]
+
+
+class CSweepSizes(ctypes.Structure):
+    _fields_ = [("words_per_config", ctypes.c_uint64), ("summary_per_config", ctypes.c_uint64),
+                ("max_layers", ctypes.c_int32)]
+
+
 # Every entry point include/tissuemc_b200.h declares: name -> (restype, argtypes)
 _P = ctypes.POINTER
 PROTOTYPES = {
@@ -121,6 +143,16 @@ PROTOTYPES = {
     "tmc_b200_parse_mci": (ctypes.c_int, [ctypes.c_char_p, _P(CRunSpec), ctypes.c_int32,
                                           _P(ctypes.c_int32), _P(CStatus)]),
     "tmc_b200_run_static": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _P(CResult), _P(CStatus)]),
+    "tmc_b200_sweep_default_options": (None, [_P(CSweepOptions)]),
+    "tmc_b200_sweep_sample": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int32, _P(CSweepConfig), _P(CStatus)]),
+    "tmc_b200_sweep_sizes": (ctypes.c_int, [_P(CSweepConfig), ctypes.c_int32, _P(CSweepOptions),
+                                            _P(CSweepSizes), _P(CStatus)]),
+    "tmc_b200_sweep_run": (ctypes.c_int, [_P(CSweepConfig), ctypes.c_int32, _P(CSweepOptions), _pu, _pd, _pd,
+                                          _P(CStatus)]),
+    "tmc_b200_sweep_run_loop": (ctypes.c_int, [_P(CSweepConfig), ctypes.c_int32, _P(CSweepOptions), _pu, _pd,
+                                               _P(CStatus)]),
+    "tmc_b200_sweep_autotune": (ctypes.c_int, [_P(CSweepConfig), ctypes.c_int32, _P(CSweepOptions), _pd,
+                                               _P(CStatus)]),
     "tmc_b200_plan": (ctypes.c_int, [_P(CRunSpec), _P(COptions), ctypes.c_int32, ctypes.c_int64,
                                      ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _P(CPlan),
                                      _P(CStatus)]),
@@ -402,3 +434,93 @@ def parse_mci(path: str | Path) -> list[RunSpec]:
 def workload(name: str) -> RunSpec:
     """A bundled workload: 'slab_n14' (one slab, 1e6 photons) or 'skin5' (five layers, 1e8)."""
     return parse_mci(CONFIGS / f"{name}.mci")[0]
+
+
+# ---------------------------------------------------------------------------------- batched sweep
+def sweep_options(**kw) -> CSweepOptions:
+    """Sweep options (grid shared by every configuration); defaults: nr = nz = 64, dr = dz = 0.01 cm,
+    na = 1, 10 batches, fast math, 256 threads, 256 photons per work item."""
+    o = CSweepOptions()
+    lib().tmc_b200_sweep_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def sweep_sample(master_seed: int, n: int):
+    """n configurations of the sweep distribution (1-3 layers, log-uniform optics, 1e4-1e6
+    photons, one seed each), as a ctypes array of CSweepConfig."""
+    arr = (CSweepConfig * n)()
+    st = CStatus()
+    _check(lib().tmc_b200_sweep_sample(master_seed, n, arr, ctypes.byref(st)), st)
+    return arr
+
+
+def sweep_config(spec: RunSpec, photons: int, seed: int) -> CSweepConfig:
+    c = CSweepConfig()
+    c.photons, c.seed, c.n_above, c.n_below = photons, seed, spec.n_above, spec.n_below
+    c.num_layers = len(spec.layers)
+    for i, lay in enumerate(spec.layers[:MAX_LAYERS]):
+        c.layers[i] = Layer(*map(float, lay))
+    return c
+
+
+def config_spec(c: CSweepConfig, opt: CSweepOptions) -> RunSpec:
+    """A sweep configuration as a single run on the sweep's grid."""
+    layers = [(c.layers[i].n, c.layers[i].mua, c.layers[i].mus, c.layers[i].g, c.layers[i].d)
+              for i in range(c.num_layers)]
+    return RunSpec(layers=layers, photons=int(c.photons), dz=opt.dz, dr=opt.dr, nz=opt.nz, nr=opt.nr, na=opt.na,
+                   n_above=c.n_above, n_below=c.n_below)
+
+
+def sweep_sizes(cfgs, opt: CSweepOptions) -> CSweepSizes:
+    sz, st = CSweepSizes(), CStatus()
+    _check(lib().tmc_b200_sweep_sizes(cfgs, len(cfgs), ctypes.byref(opt), ctypes.byref(sz), ctypes.byref(st)), st)
+    return sz
+
+
+@dataclass
+class SweepResult:
+    summary: np.ndarray  # (n, nr + 3): R_d(r) per photon, then R_d, T_t, A per photon
+    raw: np.ndarray | None  # (n, words_per_config) fixed-point tallies
+    seconds: float  # device time of the sweep kernel (or of the whole loop for run_loop)
+
+
+def sweep_run(cfgs, opt: CSweepOptions | None = None, raw: bool = False) -> SweepResult:
+    """Run every configuration in one graph-captured persistent launch."""
+    opt = opt or sweep_options()
+    sz = sweep_sizes(cfgs, opt)
+    n = len(cfgs)
+    summary = np.zeros((n, int(sz.summary_per_config)))
+    raw_arr = np.zeros((n, int(sz.words_per_config)), np.uint64) if raw else None
+    secs = ctypes.c_double(0.0)
+    st = CStatus()
+    rc = lib().tmc_b200_sweep_run(cfgs, n, ctypes.byref(opt),
+                                  raw_arr.ctypes.data_as(_pu) if raw else ctypes.cast(None, _pu),
+                                  summary.ctypes.data_as(_pd), ctypes.byref(secs), ctypes.byref(st))
+    _check(rc, st)
+    return SweepResult(summary, raw_arr, secs.value)
+
+
+def sweep_run_loop(cfgs, opt: CSweepOptions | None = None, raw: bool = False) -> SweepResult:
+    """The baseline: one single-run launch per configuration, back to back on one stream."""
+    opt = opt or sweep_options()
+    sz = sweep_sizes(cfgs, opt)
+    n = len(cfgs)
+    raw_arr = np.zeros((n, int(sz.words_per_config)), np.uint64) if raw else None
+    secs = ctypes.c_double(0.0)
+    st = CStatus()
+    rc = lib().tmc_b200_sweep_run_loop(cfgs, n, ctypes.byref(opt),
+                                       raw_arr.ctypes.data_as(_pu) if raw else ctypes.cast(None, _pu),
+                                       ctypes.byref(secs), ctypes.byref(st))
+    _check(rc, st)
+    return SweepResult(np.zeros((0, 0)), raw_arr, secs.value)
+
+
+def sweep_autotune(cfgs, opt: CSweepOptions | None = None) -> tuple[CSweepOptions, float]:
+    """Pick the sweep's block size and work-item size by timing candidates on these configurations."""
+    opt = opt or sweep_options()
+    best = ctypes.c_double(0.0)
+    st = CStatus()
+    _check(lib().tmc_b200_sweep_autotune(cfgs, len(cfgs), ctypes.byref(opt), ctypes.byref(best), ctypes.byref(st)), st)
+    return opt, best.value

@@ -19,6 +19,7 @@
 #include "../../include/tissuemc_b200.h"
 #include "walk_kernel.cuh"
 #include "engine_host.hpp"
+#include "engine_internal.hpp"
 
 namespace tmc {
 
@@ -134,7 +135,9 @@ Plan make_plan(const tmc_run_spec &spec, const tmc_options &opt, const DeviceLim
                         : std::min(lim.smem_block_optin, lim.smem_sm / static_cast<size_t>(bps) - lim.reserved);
     budget &= ~static_cast<size_t>(15);
     const size_t layer_bytes = ((static_cast<size_t>(sh.nl) * sizeof(LayerC) + 15) / 16) * 16;
-    size_t rem = budget > layer_bytes + 16 ? budget - layer_bytes - 16 : 0;
+    const size_t ring_bytes = 32 * static_cast<size_t>(p.threads);  // 8 random words per lane
+    budget = std::max(budget, layer_bytes + ring_bytes + 16);
+    size_t rem = budget - layer_bytes - ring_bytes - 16;
     const size_t batch_bytes = static_cast<size_t>(sh.nb) * (4 + sh.nl) * 8;
     p.batch_smem = batch_bytes <= rem / 4 ? 1 : 0;
     if (p.batch_smem) rem -= batch_bytes;
@@ -167,52 +170,15 @@ Plan make_plan(const tmc_run_spec &spec, const tmc_options &opt, const DeviceLim
 
 size_t plan_smem_bytes(const WalkParams &P) { return static_cast<size_t>(smem_layout(P).total) * 8; }
 
-// Fill WalkParams from a validated run (layers in float, computed as the reference does).
-WalkParams make_params(const tmc_run_spec &spec, const tmc_options &opt, const Plan &pl,
-                       unsigned long long *d_tally, unsigned long long *d_counter) {
-    const RunShape sh = shape_of(spec, opt);
-    WalkParams P{};
-    P.photons = sh.photons;
-    P.seed = opt.seed;
-    P.plan_base = sh.photons / static_cast<uint64_t>(sh.nb);
-    P.plan_extra = sh.photons % static_cast<uint64_t>(sh.nb);
-    P.nb = sh.nb;
-    P.nl = sh.nl;
-    P.nz = sh.nz;
-    P.nr = sh.nr;
-    P.na = sh.na;
-    const TallyOffsets off = tally_offsets(sh);
-    P.counter = d_counter;
-    P.g_batch = d_tally + off.batch;
-    P.g_arz = d_tally + off.a_rz;
-    P.g_rd = d_tally + off.rd_ra;
-    P.g_tt = d_tally + off.tt_ra;
-    {
-        const float n0 = static_cast<float>(spec.n_above), n1 = static_cast<float>(spec.layers[0].n);
-        const float r = (n0 - n1) / (n0 + n1);
-        P.launch_w = 1.0f - r * r;
-    }
-    P.dz = static_cast<float>(spec.dz);
-    P.dr = static_cast<float>(spec.dr);
-    P.da = static_cast<float>(0.5 * 3.14159265358979323846 / spec.na);
-    P.inv_dz = 1.0f / P.dz;
-    P.inv_dr = 1.0f / P.dr;
-    P.inv_da = 1.0f / P.da;
-    P.tr_a = pl.tr_a;
-    P.tz_a = pl.tz_a;
-    P.tr_rd = pl.tr_rd;
-    P.tr_tt = pl.tr_tt;
-    P.cross = pl.cross;
-    P.batch_smem = pl.batch_smem;
-    P.profiles = opt.profiles ? 1 : 0;
-    P.step_cap = 2000000000u;
-    P.chunk = 256;
+// Layer constants in float, computed in the same order as the reference evaluates them.
+void fill_layers(const tmc_run_spec &spec, LayerC *out) {
     double zacc = 0.0;
-    for (int i = 0; i < sh.nl; ++i) {
+    for (int i = 0; i < spec.num_layers; ++i) {
         const tmc_layer &s = spec.layers[i];
         const double nt = i == 0 ? spec.n_above : spec.layers[i - 1].n;
-        const double nb = i + 1 == sh.nl ? spec.n_below : spec.layers[i + 1].n;
-        LayerC &L = P.layers[i];
+        const double nb = i + 1 == spec.num_layers ? spec.n_below : spec.layers[i + 1].n;
+        LayerC &L = out[i];
+        L = LayerC{};
         L.mua = static_cast<float>(s.mua);
         L.mus = static_cast<float>(s.mus);
         L.mut = L.mua + L.mus;
@@ -234,15 +200,61 @@ WalkParams make_params(const tmc_run_spec &spec, const tmc_options &opt, const P
         L.cc_dn = static_cast<float>(s.n > nb ? std::sqrt(1.0 - (nb * nb) / (s.n * s.n)) : 0.0);
         L.rat_up = L.n / L.n_up;
         L.rat_dn = L.n / L.n_dn;
-        {
-            const float r = (L.n_up - L.n) / (L.n_up + L.n);
-            L.rn_up = r * r;
-        }
-        {
-            const float r = (L.n_dn - L.n) / (L.n_dn + L.n);
-            L.rn_dn = r * r;
-        }
+        const float ru = (L.n_up - L.n) / (L.n_up + L.n);
+        L.rn_up = ru * ru;
+        const float rd = (L.n_dn - L.n) / (L.n_dn + L.n);
+        L.rn_dn = rd * rd;
     }
+}
+
+// Launch weight 1 - R_sp in float, as the reference's launch() computes it (physics.hpp:50-66).
+float launch_weight(const tmc_run_spec &spec) {
+    const float n0 = static_cast<float>(spec.n_above), n1 = static_cast<float>(spec.layers[0].n);
+    const float r = (n0 - n1) / (n0 + n1);
+    return 1.0f - r * r;
+}
+
+// Fill WalkParams from a validated run.
+WalkParams make_params(const tmc_run_spec &spec, const tmc_options &opt, const Plan &pl,
+                       unsigned long long *d_tally, unsigned int *d_counter) {
+    const RunShape sh = shape_of(spec, opt);
+    WalkParams P{};
+    P.photons = sh.photons;
+    P.seed = opt.seed;
+    P.plan_base = static_cast<uint32_t>(sh.photons / static_cast<uint64_t>(sh.nb));
+    P.plan_extra = static_cast<uint32_t>(sh.photons % static_cast<uint64_t>(sh.nb));
+    P.plan_bnd = P.plan_extra * (P.plan_base + 1u);
+    P.threads = static_cast<uint32_t>(pl.threads);
+    P.nb = sh.nb;
+    P.nl = sh.nl;
+    P.nz = sh.nz;
+    P.nr = sh.nr;
+    P.na = sh.na;
+    const TallyOffsets off = tally_offsets(sh);
+    P.counter = d_counter;
+    P.g_batch = d_tally + off.batch;
+    P.g_arz = d_tally + off.a_rz;
+    P.g_rd = d_tally + off.rd_ra;
+    P.g_tt = d_tally + off.tt_ra;
+    P.launch_w = launch_weight(spec);
+    P.dz = static_cast<float>(spec.dz);
+    P.dr = static_cast<float>(spec.dr);
+    P.da = static_cast<float>(0.5 * 3.14159265358979323846 / spec.na);
+    P.inv_dz = 1.0f / P.dz;
+    P.inv_dr = 1.0f / P.dr;
+    P.inv_da = 1.0f / P.da;
+    P.tr_a = pl.tr_a;
+    P.tz_a = pl.tz_a;
+    P.tr_rd = pl.tr_rd;
+    P.tr_tt = pl.tr_tt;
+    P.cross = pl.cross;
+    P.batch_smem = pl.batch_smem;
+    P.profiles = opt.profiles ? 1 : 0;
+    P.step_cap = 2000000000u;
+    // ids a warp claims at once: one per lane, so that when the ids run out no warp is left holding
+    // a backlog of unstarted photons while others idle
+    P.chunk = 32;
+    fill_layers(spec, P.layers);
     return P;
 }
 
@@ -260,7 +272,7 @@ void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
     else
         TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&regs_bps, walk_kernel<0>, threads, 0));
     const Plan pl = make_plan(spec, opt, limits_of(c.prop), regs_bps);
-    WalkParams P = make_params(spec, opt, pl, d_tally, c.d_counter);
+    WalkParams P = make_params(spec, opt, pl, d_tally, reinterpret_cast<unsigned int *>(c.d_counter));
     const size_t smem = plan_smem_bytes(P);
     if (smem > c.prop.sharedMemPerBlockOptin)
         throw Fail(TMC_BAD_CONFIG, "the tally plan does not fit in shared memory");
@@ -279,6 +291,27 @@ void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
 }
 
 }  // namespace
+
+double run_single_loop(const tmc_run_spec *specs, const tmc_options *opts, int n, std::vector<uint64_t> *raw,
+                       std::vector<size_t> *offsets) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    std::vector<size_t> off(static_cast<size_t>(n) + 1, 0);
+    for (int c = 0; c < n; ++c) off[c + 1] = off[c] + tally_offsets(shape_of(specs[c], opts[c])).total;
+    DeviceCtx &c = device_ctx(opts[0].device);
+    ensure_tally(c, off[n]);
+    TMC_CUDA(cudaEventRecord(c.ev0, c.stream));
+    for (int i = 0; i < n; ++i) launch_walk(specs[i], opts[i], c, c.d_tally + off[i], c.stream, nullptr, nullptr);
+    TMC_CUDA(cudaEventRecord(c.ev1, c.stream));
+    TMC_CUDA(cudaStreamSynchronize(c.stream));
+    float ms = 0.f;
+    TMC_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+    if (raw) {
+        raw->resize(off[n]);
+        TMC_CUDA(cudaMemcpy(raw->data(), c.d_tally, off[n] * 8, cudaMemcpyDeviceToHost));
+    }
+    if (offsets) *offsets = off;
+    return static_cast<double>(ms) / 1000.0;
+}
 // ------------------------------------------------------------- allocation-free entry point
 // Some callers cannot allocate device memory: a host program that runs while a CUDA stream is
 // being captured into a graph (cudaMalloc is not permitted during capture), or a framework that
@@ -436,7 +469,7 @@ int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_re
         else
             TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&regs_bps, walk_kernel<0>, threads, 0));
         const Plan pl = make_plan(*spec, *opt, limits_of(d.prop), regs_bps);
-        WalkParams P = make_params(*spec, *opt, pl, tally, counter);
+        WalkParams P = make_params(*spec, *opt, pl, tally, reinterpret_cast<unsigned int *>(counter));
         const size_t smem = plan_smem_bytes(P);
         if (smem > d.prop.sharedMemPerBlockOptin)
             throw Fail(TMC_BAD_CONFIG, "the tally plan does not fit in shared memory");

@@ -1,0 +1,239 @@
+// The batched sweep: thousands of independent tissue configurations in one persistent launch.
+//
+// No reference code exists for this (it is an addition of this engine); each configuration's
+// photons follow exactly the single-run walk (walk_step.cuh) with the Philox key of that
+// configuration, so a configuration's tallies are bit for bit those of a single run with the
+// same seed, photons, batches and grid.
+//
+// Work is a queue of items (configuration, first photon, count): configuration c's photons in
+// chunks of item_photons, numbered through a prefix sum and taken in a strided permutation of
+// that numbering, so that the warps at work at any moment are spread over many configurations
+// (their tallies then rarely meet on one L2 line). A warp takes items one at a time and hands their
+// photons to its idle lanes; every lane carries the
+// configuration of its own photon (Philox key, layer table pointer, tally base), so a warp moves
+// on to the next item while some of its lanes still finish photons of the previous one, and no
+// lane waits for an item to drain. Tallies of configuration c live at tally + c * stride in the
+// single-run layout (batch totals, A(r,z), R_d(r,a), T_t(r,a)), accumulated with 64-bit integer
+// atomics in global memory (L2); a per-lane run cache merges consecutive deposits into one bin.
+#pragma once
+
+#include "walk_step.cuh"
+
+namespace tmc {
+
+// One configuration, as the kernel reads it.
+struct SweepConfigC {
+    uint32_t photons, plan_base, plan_extra, plan_bnd;  // photons and their BatchPlan
+    uint32_t k0, k1;                                     // Philox key: this configuration's seed
+    float launch_w;                                      // 1 - specular reflectance (float)
+    int nl;                                              // layers
+    int layer_base;                                      // index of layer 0 in the layer table
+    int pad[3];
+};
+static_assert(sizeof(SweepConfigC) == 48, "SweepConfigC layout");
+
+// Per-sweep header in device memory (written by the sweep's host-to-device copy, so that one
+// captured graph serves sweeps of different sizes).
+struct SweepHeader {
+    uint32_t n_cfg;         // configurations
+    uint32_t total_items;   // work items: configuration c has ceil(photons_c / item_photons)
+    uint32_t perm;          // items are taken in the order j = i * perm mod total_items
+    uint32_t item_photons;  // photons per item (the last item of a configuration may hold fewer)
+};
+
+struct SweepParams {
+    const SweepHeader *hdr;
+    const SweepConfigC *cfgs;
+    const uint32_t *prefix;         // [n_cfg + 1] first item of each configuration
+    const LayerC *layers;
+    unsigned int *item_counter;     // next unclaimed item (zeroed before launch)
+    unsigned long long *tally;      // [configs * stride]
+    int stride;                     // 64-bit words per configuration
+    int nb, lmax, nz, nr, na;       // batches, layer slots per batch row, grid
+    float dz, dr, da, inv_dz, inv_dr, inv_da;
+    int profiles;
+    uint32_t step_cap;
+    uint32_t threads;
+};
+
+template <int FAST> struct SweepCtx {
+    const SweepParams &P;
+    Ring ring;
+    uint32_t step_cap;
+    int a_off, rd_off, tt_off, bstride;  // word offsets inside one configuration's tallies
+    // the configuration of this lane's current photon
+    uint32_t k0, k1;
+    int nl;
+    const LayerC *layers;
+    unsigned long long *t;
+    // run cache: word index into P.tally of the last A(r,z) bin, and its pending value
+    int cache_key;
+    unsigned long long cache_val;
+
+    __device__ __forceinline__ void refill(Lane &L) const { ring.refill(L, k0, k1); }
+    __device__ __forceinline__ uint32_t draw(Lane &L) const { return ring.draw(L); }
+    __device__ __forceinline__ const LayerC &layer(const Lane &, int l) const { return layers[l]; }
+    __device__ __forceinline__ int num_layers(const Lane &) const { return nl; }
+    __device__ __forceinline__ void batch_add(const Lane &L, int slot, unsigned long long v) const {
+        atomicAdd(&t[L.batch * bstride + slot], v);
+    }
+    __device__ __forceinline__ void absorb(const Lane &L, unsigned long long v) {
+        if (!P.profiles) return;
+        const float rr = m_sqrt<FAST>(L.x * L.x + L.y * L.y);
+        const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
+        const int iz = bin_of<FAST>(L.z, P.dz, P.inv_dz, P.nz);
+        const int key = static_cast<int>(t - P.tally) + a_off + ir * P.nz + iz;
+        if (key == cache_key) {
+            cache_val += v;
+        } else {
+            if (cache_key >= 0) atomicAdd(&P.tally[cache_key], cache_val);
+            cache_key = key;
+            cache_val = v;
+        }
+    }
+    __device__ __forceinline__ void flush_cache() {
+        if (cache_key >= 0) atomicAdd(&P.tally[cache_key], cache_val);
+        cache_key = -1;
+    }
+    __device__ __forceinline__ void exit(const Lane &L, int kind, unsigned long long v) const {
+        if (!P.profiles) return;
+        const float rr = m_sqrt<FAST>(L.x * L.x + L.y * L.y);
+        const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
+        const int ia = P.na > 1 ? bin_of<FAST>(acosf(fminf(fabsf(L.uz), 1.0f)), P.da, P.inv_da, P.na) : 0;
+        atomicAdd(&t[(kind == 1 ? rd_off : tt_off) + ir * P.na + ia], v);
+    }
+};
+
+// Minimum resident 256-thread blocks per SM the compiler must allow for (0: no bound).
+#ifndef TMC_SWEEP_MIN_BLOCKS
+#define TMC_SWEEP_MIN_BLOCKS 0
+#endif
+#if TMC_SWEEP_MIN_BLOCKS > 0
+#define TMC_SWEEP_BOUNDS __launch_bounds__(256, TMC_SWEEP_MIN_BLOCKS)
+#else
+#define TMC_SWEEP_BOUNDS __launch_bounds__(256)
+#endif
+
+template <int FAST>
+__global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParams P) {
+    extern __shared__ __align__(16) unsigned long long smem[];
+    SweepCtx<FAST> C{P,
+                     Ring{reinterpret_cast<uint32_t *>(smem) + threadIdx.x, static_cast<int>(P.threads)},
+                     P.step_cap,
+                     P.nb * (4 + P.lmax),
+                     P.nb * (4 + P.lmax) + P.nr * P.nz,
+                     P.nb * (4 + P.lmax) + P.nr * P.nz + P.nr * P.na,
+                     4 + P.lmax,
+                     0u,
+                     0u,
+                     1,
+                     P.layers,
+                     P.tally,
+                     -1,
+                     0ull};
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const SweepHeader H = *P.hdr;
+
+    // warp-uniform: the item being handed out
+    uint32_t it_cfg = 0u, it_next = 0u, it_end = 0u;
+    bool items_done = false;
+    unsigned ex_mask = 0u;  // warp-uniform: lanes with no photon left to take
+    bool alive = false;
+    Lane L;
+
+    for (;;) {
+        unsigned need = ~__ballot_sync(0xffffffffu, alive) & ~ex_mask;
+        while (need) {  // warp-uniform: hand out photons, taking new items as they run out
+            const uint32_t avail = it_end - it_next;
+            if (avail == 0u) {
+                if (!items_done) {
+                    const int leader = __ffs(need) - 1;
+                    uint32_t idx = 0u;
+                    if (static_cast<int>(lane) == leader) idx = atomicAdd(P.item_counter, 1u);
+                    idx = __shfl_sync(0xffffffffu, idx, leader);
+                    if (idx < H.total_items) {
+                        const uint32_t j = static_cast<uint32_t>(
+                            (static_cast<uint64_t>(idx) * H.perm) % H.total_items);
+                        uint32_t lo = 0u, hi = H.n_cfg;  // the c with prefix[c] <= j < prefix[c + 1]
+                        while (hi - lo > 1u) {
+                            const uint32_t mid = (lo + hi) >> 1;
+                            if (P.prefix[mid] <= j) lo = mid;
+                            else hi = mid;
+                        }
+                        const uint32_t first = (j - P.prefix[lo]) * H.item_photons;
+                        const uint32_t left = P.cfgs[lo].photons - first;
+                        it_cfg = lo;
+                        it_next = first;
+                        it_end = first + (left < H.item_photons ? left : H.item_photons);
+                        continue;
+                    }
+                    items_done = true;
+                }
+                ex_mask |= need;
+                break;
+            }
+            const uint32_t n = static_cast<uint32_t>(__popc(need));
+            const uint32_t take = n < avail ? n : avail;
+            const uint32_t rank = static_cast<uint32_t>(__popc(need & lt_mask));
+            const bool mine = ((need >> lane) & 1u) && rank < take;
+            if (mine) {
+                const SweepConfigC cf = P.cfgs[it_cfg];
+                const uint32_t id = it_next + rank;
+                C.k0 = cf.k0;
+                C.k1 = cf.k1;
+                C.nl = cf.nl;
+                C.layers = P.layers + cf.layer_base;
+                C.t = P.tally + static_cast<size_t>(it_cfg) * static_cast<size_t>(P.stride);
+                const int batch = static_cast<int>(id < cf.plan_bnd ? id / (cf.plan_base + 1u)
+                                                                    : cf.plan_extra + (id - cf.plan_bnd) / cf.plan_base);
+                launch(L, C, id, batch, cf.launch_w);
+                alive = true;
+            }
+            need &= ~__ballot_sync(0xffffffffu, mine);
+            it_next += take;
+        }
+        if (ex_mask == 0xffffffffu) break;  // exhausted lanes hold no photon: the warp is done
+        if (!alive) continue;
+        if (walk_step<FAST>(L, C)) alive = false;
+    }
+    C.flush_cache();
+}
+
+// Per-configuration summaries from the integer tallies, in double: R_d(r) per photon (nr values,
+// summed over exit angles), then total R_d, T_t and absorbed weight per photon. One warp per
+// configuration; deterministic (integer sums, converted once).
+__global__ void sweep_finalize_kernel(const SweepConfigC *cfgs, const unsigned long long *tally, int n_cfg,
+                                      int stride, int nb, int lmax, int nz, int nr, int na, double *summary) {
+    const int warp = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= n_cfg) return;
+    const unsigned long long *t = tally + static_cast<size_t>(warp) * stride;
+    const int bstride = 4 + lmax;
+    const int rd_off = nb * bstride + nr * nz;
+    const double k = 1.0 / (4294967296.0 * static_cast<double>(cfgs[warp].photons));
+    double *out = summary + static_cast<size_t>(warp) * (nr + 3);
+    for (int ir = lane; ir < nr; ir += 32) {
+        unsigned long long s = 0ull;
+        for (int ia = 0; ia < na; ++ia) s += t[rd_off + ir * na + ia];
+        out[ir] = static_cast<double>(s) * k;
+    }
+    unsigned long long rd = 0ull, tt = 0ull, ab = 0ull;
+    for (int b = lane; b < nb; b += 32) {
+        rd += t[b * bstride + 0];
+        tt += t[b * bstride + 1];
+        for (int l = 0; l < lmax; ++l) ab += t[b * bstride + 4 + l];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        rd += __shfl_down_sync(0xffffffffu, rd, o);
+        tt += __shfl_down_sync(0xffffffffu, tt, o);
+        ab += __shfl_down_sync(0xffffffffu, ab, o);
+    }
+    if (lane == 0) {
+        out[nr] = static_cast<double>(rd) * k;
+        out[nr + 1] = static_cast<double>(tt) * k;
+        out[nr + 2] = static_cast<double>(ab) * k;
+    }
+}
+
+}  // namespace tmc

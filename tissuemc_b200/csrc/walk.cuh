@@ -42,11 +42,13 @@ static_assert(sizeof(LayerC) == 24 * 4, "LayerC layout");
 
 // Everything the walk kernel needs, passed by value (__grid_constant__).
 struct WalkParams {
-    uint64_t photons;      // photon ids [0, photons)
+    uint64_t photons;      // photon ids [0, photons), at most 2^31
     uint64_t seed;         // Philox key
-    uint64_t plan_base;    // BatchPlan: photons per batch before the remainder
-    uint64_t plan_extra;   // BatchPlan: the first `extra` batches hold one more
-    unsigned long long *counter;   // next unclaimed photon id (zeroed before launch)
+    uint32_t plan_base;    // BatchPlan: photons per batch before the remainder
+    uint32_t plan_extra;   // BatchPlan: the first `extra` batches hold one more
+    uint32_t plan_bnd;     // BatchPlan: ids below extra * (base + 1) are in the larger batches
+    uint32_t threads;      // block size (the random-word ring's stride)
+    unsigned int *counter; // next unclaimed photon id (zeroed before launch)
     unsigned long long *g_batch;   // [nb * (4 + nl)] rd, tt, events, anomalies, absorbed[nl]
     unsigned long long *g_arz;     // [nr * nz]
     unsigned long long *g_rd;      // [nr * na]
@@ -140,11 +142,5 @@ __device__ __forceinline__ unsigned long long to_fixed(float w) {
     return __float2ull_rn(w * kFixedScale);
 }
 
-// Clamped bin index (src/cpu/engine.cpp:59-66): non-positive (or NaN) -> 0, beyond -> last.
-__device__ __forceinline__ int clamp_bin(float x, float inv_width, int count) {
-    if (!(x > 0.0f)) return 0;
-    const float i = x * inv_width;
-    return i >= static_cast<float>(count) ? count - 1 : static_cast<int>(i);
-}
 
 }  // namespace tmc

@@ -1,0 +1,303 @@
+// One MCML step of one lane, shared by the single-run kernel (walk_kernel.cuh) and the
+// multi-configuration sweep kernel (sweep_kernel.cuh).
+//
+// Step semantics: TissueMC's include/tissuemc/physics.hpp — step size :148-158, boundary distance
+// :162-178, hop :180-184, drop :187-193, Henyey-Greenstein :101-113, spin :116-144, Fresnel
+// :71-98, crossing :198-246, roulette :250-259, step_once :263-277. A kernel supplies a context
+// `Ctx` that says where the layer table and the tallies live:
+//   ctx.refill(lane)          append the lane's next Philox block to its random-word ring
+//   ctx.draw(lane)            next random word
+//   ctx.layer(lane, l)        constants of layer l of the lane's tissue
+//   ctx.num_layers(lane)
+//   ctx.absorb(lane, v)       score an absorption of v (fixed point) at the lane's position
+//   ctx.exit(lane, kind, v)   score an exit (1: reflectance, 2: transmittance) of v
+//   ctx.batch_add(lane, i, v) add v to slot i of the lane's batch totals
+//   ctx.step_cap              steps after which a packet is ended as an anomaly
+#pragma once
+
+#include "walk.cuh"
+
+namespace tmc {
+
+constexpr float kCosZero = 1.0f - 1e-6f;  // physics.hpp:35 (float widening of MCML COSZERO)
+constexpr float kCos90D = 1e-6f;          // physics.hpp:36
+constexpr float kWeightMin = 1e-4f;       // physics.hpp:33 (MCML WEIGHT)
+constexpr float kChance = 0.1f;           // physics.hpp:34 (MCML CHANCE)
+constexpr float kTwoPi = 2.0f * 3.14159265358979323846f;  // evaluated as the reference does
+
+// Register copy of the current layer's constants used on every step.
+struct Hot {
+    float mua, mut, inv_mut, absorb, z0, z1, g, hg_a, hg_b, hg_c, hg_d, inv_2g;
+};
+
+__device__ __forceinline__ void load_hot(Hot &h, const LayerC &L) {
+    h.mua = L.mua;
+    h.mut = L.mut;
+    h.inv_mut = L.inv_mut;
+    h.absorb = L.absorb;
+    h.z0 = L.z0;
+    h.z1 = L.z1;
+    h.g = L.g;
+    h.hg_a = L.hg_a;
+    h.hg_b = L.hg_b;
+    h.hg_c = L.hg_c;
+    h.hg_d = L.hg_d;
+    h.inv_2g = L.inv_2g;
+}
+
+// Fresnel reflectance for unpolarised light from index n1 into n2 at cos(incidence) ca1
+// (physics.hpp:71-98); rn is the precomputed normal-incidence value and rat = n1 / n2.
+template <int FAST>
+__device__ __forceinline__ float fresnel(float n1, float n2, float ca1, float rn, float rat,
+                                         float &ca2) {
+    if (n1 == n2) {
+        ca2 = ca1;
+        return 0.0f;
+    }
+    if (ca1 > kCosZero) {
+        ca2 = ca1;
+        return rn;
+    }
+    if (ca1 < kCos90D) {
+        ca2 = 0.0f;
+        return 1.0f;
+    }
+    const float sa1 = m_sqrt<FAST>(1.0f - ca1 * ca1);
+    float sa2;
+    if constexpr (Math<FAST>::div) sa2 = sa1 * rat;
+    else sa2 = n1 * sa1 / n2;
+    if (sa2 >= 1.0f) {
+        ca2 = 0.0f;
+        return 1.0f;
+    }
+    ca2 = m_sqrt<FAST>(1.0f - sa2 * sa2);
+    const float cap = ca1 * ca2 - sa1 * sa2;
+    const float cam = ca1 * ca2 + sa1 * sa2;
+    const float sap = sa1 * ca2 + ca1 * sa2;
+    const float sam = sa1 * ca2 - ca1 * sa2;
+    return m_div<FAST>(0.5f * sam * sam * (cam * cam + cap * cap), sap * sap * cam * cam);
+}
+
+// Clamped bin index (src/cpu/engine.cpp:59-66 semantics, branch-free): x <= 0 or NaN -> 0,
+// x / width >= n -> n - 1, else floor(x / width).
+template <int FAST> __device__ __forceinline__ int bin_of(float x, float width, float inv_width, int n) {
+    float i;
+    if constexpr (Math<FAST>::div) i = x * inv_width;
+    else i = x / width;
+    return static_cast<int>(fminf(fmaxf(i, 0.0f), static_cast<float>(n - 1)));
+}
+
+// All state of one lane's current photon (registers).
+struct Lane {
+    float x, y, z, ux, uy, uz, w, sleft;
+    int layer, batch;
+    uint32_t id, blk, rp, wp;  // photon id, Philox block, ring read/write positions
+    uint32_t events, anomalies, steps;
+    unsigned long long run_abs;  // fixed-point weight absorbed in the current layer
+    Hot h;
+};
+
+// Launch a packet at the origin, straight down, in layer 0 (physics.hpp:58-66).
+template <class Ctx>
+__device__ __forceinline__ void launch(Lane &L, Ctx &C, uint32_t id, int batch, float launch_w) {
+    L.id = id;
+    L.blk = 0u;
+    L.rp = L.wp = 0u;
+    L.x = L.y = L.z = 0.f;
+    L.ux = L.uy = 0.f;
+    L.uz = 1.f;
+    L.w = launch_w;
+    L.sleft = 0.f;
+    L.layer = 0;
+    load_hot(L.h, C.layer(L, 0));
+    L.batch = batch;
+    L.events = L.anomalies = L.steps = 0u;
+    L.run_abs = 0ull;
+}
+
+// One hop-drop-spin (or boundary) step plus roulette; returns true when the packet has ended
+// (its per-photon totals are then published).
+template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L, Ctx &C) {
+    if (L.wp - L.rp < 4u) C.refill(L);  // a step draws at most 4 words
+    ++L.steps;
+    float s;
+    if (L.sleft == 0.0f) {
+        const float u = unit_open(C.draw(L));
+        if constexpr (Math<FAST>::log) {
+            // the SFU logarithm's absolute error can flip the sign of log(u) for the two largest
+            // u of the 23-bit grid; a step is never negative
+            s = fmaxf(-m_log<FAST>(u), 0.0f) * L.h.inv_mut;
+        } else if constexpr (Math<FAST>::div) {
+            s = -m_log<FAST>(u) * L.h.inv_mut;
+        } else {
+            s = -m_log<FAST>(u) / L.h.mut;
+        }
+    } else {
+        if constexpr (Math<FAST>::div) s = L.sleft * L.h.inv_mut;
+        else s = L.sleft / L.h.mut;
+        L.sleft = 0.0f;
+    }
+    bool hit = false;
+    if (L.uz != 0.0f) {
+        const float db = m_div<FAST>((L.uz > 0.0f ? L.h.z1 : L.h.z0) - L.z, L.uz);
+        if (s > db) {
+            L.sleft = (s - db) * L.h.mut;
+            s = db;
+            hit = true;
+        }
+    }
+    L.x += s * L.ux;
+    L.y += s * L.uy;
+    L.z += s * L.uz;
+
+    bool died = false;
+    int exit_kind = 0;  // 1: reflectance (top), 2: transmittance (bottom)
+    if (hit) {
+        // ---- boundary: reflect, or transmit into the next layer or out (physics.hpp:198-246)
+        const LayerC &Lc = C.layer(L, L.layer);
+        const bool up = L.uz < 0.0f;
+        const float ca1 = up ? -L.uz : L.uz;
+        const float nt = up ? Lc.n_up : Lc.n_dn;
+        const float rat = up ? Lc.rat_up : Lc.rat_dn;
+        float uz1 = 0.0f;
+        const float r = (ca1 <= (up ? Lc.cc_up : Lc.cc_dn))
+                            ? 1.0f
+                            : fresnel<FAST>(Lc.n, nt, ca1, up ? Lc.rn_up : Lc.rn_dn, rat, uz1);
+        if (unit_open(C.draw(L)) > r) {
+            L.ux *= rat;
+            L.uy *= rat;
+            L.uz = up ? -uz1 : uz1;
+            if (up ? L.layer == 0 : L.layer == C.num_layers(L) - 1) {
+                exit_kind = up ? 1 : 2;
+                died = true;
+            } else {
+                if (L.run_abs) {
+                    C.batch_add(L, 4 + L.layer, L.run_abs);
+                    L.run_abs = 0ull;
+                }
+                L.layer += up ? -1 : 1;
+                load_hot(L.h, C.layer(L, L.layer));
+            }
+        } else {
+            L.uz = -L.uz;
+        }
+    } else {
+        // ---- drop (physics.hpp:187-193) and score the absorption
+        float dwa;
+        if constexpr (Math<FAST>::div) dwa = L.w * L.h.absorb;
+        else dwa = L.w * L.h.mua / L.h.mut;
+        L.w -= dwa;
+        ++L.events;
+        {
+            const float n2 = L.ux * L.ux + L.uy * L.uy + L.uz * L.uz;
+            if (!(dwa == dwa) || !(fabsf(n2 - 1.0f) <= 1e-5f)) ++L.anomalies;
+        }
+        const unsigned long long v = to_fixed(dwa);
+        L.run_abs += v;
+        C.absorb(L, v);
+        // ---- spin (physics.hpp:101-144)
+        float ct;
+        {
+            const float xi = unit_open(C.draw(L));
+            if (L.h.g == 0.0f) {
+                ct = 2.0f * xi - 1.0f;
+            } else {
+                const float t = m_div<FAST>(L.h.hg_a, L.h.hg_b + L.h.hg_c * xi);
+                if constexpr (Math<FAST>::div) ct = (L.h.hg_d - t * t) * L.h.inv_2g;
+                else ct = (L.h.hg_d - t * t) / L.h.hg_c;
+                ct = fminf(fmaxf(ct, -1.0f), 1.0f);
+            }
+        }
+        float st = 1.0f - ct * ct;
+        st = st > 0.0f ? m_sqrt<FAST>(st) : 0.0f;
+        float sp, cp;
+        {
+            const float u = unit_open(C.draw(L));
+            if constexpr (Math<FAST>::sincos) {
+                // psi - pi lies in (-pi, pi), where the SFU sine and cosine are accurate
+                __sincosf(kTwoPi * (u - 0.5f), &sp, &cp);
+                sp = -sp;
+                cp = -cp;
+            } else {
+                sincosf(kTwoPi * u, &sp, &cp);
+            }
+        }
+        if (fabsf(L.uz) > kCosZero) {
+            L.ux = st * cp;
+            L.uy = st * sp;
+            L.uz = L.uz >= 0.0f ? ct : -ct;
+        } else {
+            const float ox = L.ux, oy = L.uy, oz = L.uz;
+            if constexpr (Math<FAST>::sqrt) {
+                const float it = rsqrtf(1.0f - oz * oz);
+                L.ux = st * (ox * oz * cp - oy * sp) * it + ox * ct;
+                L.uy = st * (oy * oz * cp + ox * sp) * it + oy * ct;
+                L.uz = -st * cp * (1.0f - oz * oz) * it + oz * ct;
+            } else {
+                const float tmp = sqrtf(1.0f - oz * oz);
+                L.ux = st * (ox * oz * cp - oy * sp) / tmp + ox * ct;
+                L.uy = st * (oy * oz * cp + ox * sp) / tmp + oy * ct;
+                L.uz = -st * cp * tmp + oz * ct;
+            }
+        }
+        const float inv = m_rsqrt<FAST>(L.ux * L.ux + L.uy * L.uy + L.uz * L.uz);
+        L.ux *= inv;
+        L.uy *= inv;
+        L.uz *= inv;
+    }
+
+    if (exit_kind) {
+        // ---- score the exit (check, totals, R_d(r,a) or T_t(r,a))
+        const float n2 = L.ux * L.ux + L.uy * L.uy + L.uz * L.uz;
+        if (!(L.w == L.w) || !(fabsf(n2 - 1.0f) <= 1e-5f)) ++L.anomalies;
+        const unsigned long long v = to_fixed(L.w);
+        C.batch_add(L, exit_kind - 1, v);
+        C.exit(L, exit_kind, v);
+    } else if (L.w < kWeightMin) {
+        // ---- roulette (physics.hpp:250-259)
+        if (L.w == 0.0f) {
+            died = true;
+        } else if (unit_open(C.draw(L)) < kChance) {
+            if constexpr (Math<FAST>::div) L.w *= 10.0f;
+            else L.w /= kChance;
+        } else {
+            died = true;
+        }
+    }
+    if (!died && L.steps >= C.step_cap) {  // a packet that never ends is an anomaly, not a hang
+        ++L.anomalies;
+        died = true;
+    }
+    if (died) {
+        C.batch_add(L, 2, static_cast<unsigned long long>(L.events));
+        if (L.anomalies) C.batch_add(L, 3, static_cast<unsigned long long>(L.anomalies));
+        if (L.run_abs) C.batch_add(L, 4 + L.layer, L.run_abs);
+    }
+    return died;
+}
+
+// The random-word ring: 8 words per lane in shared memory, slot k of a block's lanes contiguous
+// (ring[k * stride]), so lanes reading different slots never conflict on a bank.
+struct Ring {
+    uint32_t *base;  // this lane's slot 0
+    int stride;      // lanes per block
+
+    __device__ __forceinline__ uint32_t draw(Lane &L) const {
+        const uint32_t o = base[(L.rp & 7u) * stride];
+        ++L.rp;
+        return o;
+    }
+    __device__ __forceinline__ void refill(Lane &L, uint32_t k0, uint32_t k1) const {
+        uint32_t b0, b1, b2, b3;
+        philox4x32_10(L.id, 0u, L.blk, k0, k1, b0, b1, b2, b3);
+        ++L.blk;
+        uint32_t *const slot = base + (L.wp & 4u) * stride;  // wp is a multiple of 4
+        slot[0] = b0;
+        slot[stride] = b1;
+        slot[2 * stride] = b2;
+        slot[3 * stride] = b3;
+        L.wp += 4u;
+    }
+};
+
+}  // namespace tmc
