@@ -263,6 +263,51 @@ TMC_B200_API int tmc_b200_sweep_run_loop(const tmc_sweep_config *cfgs, int32_t n
 TMC_B200_API int tmc_b200_sweep_autotune(const tmc_sweep_config *cfgs, int32_t n, tmc_sweep_options *opt,
                                          double *best_seconds, tmc_status *status);
 
+/* ------------------------------------------------------------------ tensor-core GEMM
+ * D = A * B^T (+ bias) on the tcgen05 tensor cores: A is M x K and B is N x K, BF16, row-major with
+ * K contiguous; D is M x N float32 row-major; bias (optional) has N entries; K a positive multiple
+ * of 64. All pointers are device memory of the current device; runs on `stream` and synchronises
+ * it. No counterpart in the reference (the surrogate's building block). TMC_DEVICE_TIMEOUT if a
+ * bounded tensor-core wait gave up. */
+TMC_B200_API int tmc_b200_gemm_bf16(const uint16_t *A, const uint16_t *B, const float *bias, float *D, int32_t M,
+                                    int32_t N, int32_t K, void *stream, tmc_status *status);
+
+/* ------------------------------------------------------------------ surrogate network ops
+ * The learned surrogate's building blocks (no counterpart in the reference). Device pointers of
+ * the current device; launched on `stream` without synchronising, so a training step can be
+ * captured in a CUDA graph. Matrices are row-major; "bf16" buffers are uint16_t bit patterns.
+ * Every product runs on the tcgen05 tensor cores with FP32 accumulation (K multiple of 64).
+ *
+ * linear:        Z = X W^T + b (float32, optional), H = gelu(Z) or Z (bf16, optional);
+ *                X: M x K, W: N x K, b: N.
+ * backward_data: dX = (dZ WT^T) * gelu'(Zprev) (bf16); dZ: M x K, WT: N x K (the transposed
+ *                weight, N = the layer's inputs), Zprev: M x N.
+ * matmul_f32:    D = A B^T (float32); A: M x K, B: N x K (weight gradients from transposed
+ *                activations).
+ * transpose:     Y = X^T for a rows x cols bf16 matrix.
+ * colsum:        db[n] = sum_m dZ[m][n] (float32, overwritten).
+ * mse:           loss += scale * sum (pred - target)^2 over the first T of ld columns; dZ (bf16,
+ *                optional) = 2 scale (pred - target), zero in the padded columns.
+ * adam:          one Adam step (lr_t already bias-corrected) on float32 master weights, writing
+ *                the bf16 copy wb and its transpose wt (each optional).
+ * status:        nonzero if a bounded tensor-core wait gave up since the last clear. */
+TMC_B200_API int tmc_b200_nn_linear(const uint16_t *X, const uint16_t *W, const float *bias, float *Z, uint16_t *H,
+                                    int32_t M, int32_t N, int32_t K, int32_t gelu, void *stream, tmc_status *status);
+TMC_B200_API int tmc_b200_nn_backward_data(const uint16_t *dZ, const uint16_t *WT, const float *Zprev, uint16_t *dX,
+                                           int32_t M, int32_t N, int32_t K, void *stream, tmc_status *status);
+TMC_B200_API int tmc_b200_nn_matmul_f32(const uint16_t *A, const uint16_t *B, float *D, int32_t M, int32_t N,
+                                        int32_t K, void *stream, tmc_status *status);
+TMC_B200_API int tmc_b200_nn_transpose(const uint16_t *X, uint16_t *Y, int32_t rows, int32_t cols, void *stream,
+                                       tmc_status *status);
+TMC_B200_API int tmc_b200_nn_colsum(const uint16_t *dZ, float *db, int32_t M, int32_t N, void *stream,
+                                    tmc_status *status);
+TMC_B200_API int tmc_b200_nn_mse(const float *pred, const float *target, uint16_t *dZ, float *loss, int32_t M,
+                                 int32_t T, int32_t ld, float scale, void *stream, tmc_status *status);
+TMC_B200_API int tmc_b200_nn_adam(float *w, const float *g, float *m, float *v, int32_t rows, int32_t cols,
+                                  float lr_t, float b1, float b2, float eps, float weight_decay, uint16_t *wb,
+                                  uint16_t *wt, void *stream, tmc_status *status);
+TMC_B200_API int tmc_b200_nn_status(int32_t clear);
+
 /* Parse an MCML .mci file (the reference's parse_mci_file, src/io/mci.cpp:173-183): writes up to
  * `max_runs` runs and returns the number found in *n_runs. Errors carry the line number. */
 TMC_B200_API int tmc_b200_parse_mci(const char *path, tmc_run_spec *runs, int32_t max_runs, int32_t *n_runs,

@@ -1,0 +1,186 @@
+"""The learned surrogate (needs a GPU): the tensor-core GEMM against torch, the network's loss and
+gradients against a float64 CPU restatement (tests/mlp_reference.py), the element-wise kernels,
+training on sweep-generated data, the ensemble gate, the inverse fit, and what the network gains
+over plain Monte Carlo at equal cost."""
+
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+import pytest
+
+import tissuemc_b200 as tmc
+from mlp_reference import bf16, forward_backward
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (300, 200, 128), (4096, 66, 512), (4096, 512, 512),
+                                   (513, 1000, 192)])
+def test_tensor_core_gemm_matches_fp32_reference(M, N, K):
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    A = torch.randn(M, K, device="cuda", generator=g).bfloat16()
+    B = torch.randn(N, K, device="cuda", generator=g).bfloat16()
+    bias = torch.randn(N, device="cuda", generator=g)
+    D = tmc.gemm_bf16(A, B, bias)
+    ref = A.double() @ B.double().T + bias.double()
+    rel = ((D.double() - ref).abs().max() / ref.abs().max()).item()
+    assert rel < 2e-6, rel  # FP32 accumulation of exact BF16 products
+
+
+def test_gemm_rejects_k_not_multiple_of_64():
+    A = torch.zeros(128, 32, device="cuda", dtype=torch.bfloat16)
+    with pytest.raises(tmc.ConfigError, match="multiple of 64"):
+        tmc.gemm_bf16(A, A)
+
+
+def _member_numpy(m):
+    Ws = [bf16(w.cpu().numpy()) for w in m.W]
+    bs = [b.cpu().numpy().astype(np.float64) for b in m.b]
+    return Ws, bs
+
+
+def test_gradients_match_the_float64_cpu_restatement():
+    from tissuemc_b200 import surrogate as S
+
+    B = 128
+    m = S.Member(B, seed=3)
+    rng = np.random.default_rng(0)
+    for b in m.b:  # non-zero biases exercise the bias paths
+        b.copy_(torch.from_numpy(rng.normal(0, 0.1, b.shape[0]).astype(np.float32)))
+    Xn = np.zeros((B, S.K_IN), np.float32)
+    Xn[:, :S.N_FEAT] = rng.normal(size=(B, S.N_FEAT))
+    Y = rng.normal(size=(B, S.N_OUT)).astype(np.float32)
+    X = torch.from_numpy(Xn).cuda().bfloat16()
+    Yd = torch.from_numpy(Y).cuda()
+    stream = torch.cuda.current_stream().cuda_stream
+    scale = 1.0 / (B * S.N_OUT)
+    m.forward(X, B, stream)
+    m.backward(X, Yd, stream, scale)
+    torch.cuda.synchronize()
+    Ws, bs = _member_numpy(m)
+    loss, gW, gb, pred = forward_backward(bf16(Xn), Ws, bs, Y.astype(np.float64), S.N_OUT, scale)
+    assert math.isclose(m.loss.item(), loss, rel_tol=1e-4)
+    # a BF16 activation may round to the neighbouring value when the FP32 sums differ in the last
+    # bit, so outputs agree to a fraction of a BF16 step, not bit for bit
+    zp = m.Z[-1].cpu().numpy()
+    assert np.abs(zp - pred).max() <= 1e-2 * np.abs(pred).max()
+    for li in range(len(Ws)):
+        g_gpu, g_ref = m.gW[li].cpu().numpy(), gW[li]
+        assert np.abs(g_gpu - g_ref).max() <= 2e-2 * np.abs(g_ref).max() + 1e-9, li
+        assert np.abs(m.gb[li].cpu().numpy() - gb[li]).max() <= 2e-2 * np.abs(gb[li]).max() + 1e-9, li
+        # gradients of the zero-padded inputs and outputs stay exactly zero
+    assert not m.gW[0][:, S.N_FEAT:].any() and not m.gW[-1][S.N_OUT:].any()
+
+
+def test_adam_transpose_and_colsum_kernels():
+    from tissuemc_b200 import surrogate as S
+
+    rows, cols = 96, 200
+    w = torch.randn(rows, cols, device="cuda")
+    g = torch.randn(rows, cols, device="cuda")
+    m = torch.zeros_like(w)
+    v = torch.zeros_like(w)
+    wb = torch.empty(rows, cols, dtype=torch.bfloat16, device="cuda")
+    wt = torch.empty(cols, rows, dtype=torch.bfloat16, device="cuda")
+    w0 = w.clone()
+    s = torch.cuda.current_stream().cuda_stream
+    import ctypes
+
+    S._call("tmc_b200_nn_adam", S._p(w), S._p(g), S._p(m), S._p(v), rows, cols, ctypes.c_float(0.01),
+            ctypes.c_float(0.9), ctypes.c_float(0.999), ctypes.c_float(1e-8), ctypes.c_float(0.0), S._p(wb),
+            S._p(wt), ctypes.c_void_p(s))
+    torch.cuda.synchronize()
+    mi = 0.1 * g
+    vi = 0.001 * g * g
+    ref = w0 - 0.01 * mi / (vi.sqrt() + 1e-8)
+    assert torch.allclose(w, ref, rtol=1e-5, atol=1e-6)
+    assert torch.equal(wb, w.bfloat16()) and torch.equal(wt, w.bfloat16().t())
+    x = torch.randn(300, 70, device="cuda").bfloat16()
+    y = torch.empty(70, 300, dtype=torch.bfloat16, device="cuda")
+    S._call("tmc_b200_nn_transpose", S._p(x), S._p(y), 300, 70, ctypes.c_void_p(s))
+    db = torch.empty(70, device="cuda")
+    S._call("tmc_b200_nn_colsum", S._p(x), S._p(db), 300, 70, ctypes.c_void_p(s))
+    torch.cuda.synchronize()
+    assert torch.equal(y, x.t())
+    assert torch.allclose(db, x.float().sum(0), rtol=1e-5, atol=1e-4)
+
+
+@pytest.fixture(scope="module")
+def trained():
+    """A small ensemble trained on 2^14 sweep solves at 1e4 photons (fast; the full-size run is in
+    bench.py --workload surrogate)."""
+    from tissuemc_b200 import surrogate as S
+
+    cfgs, X, Y = S.generate(16384, 10_000, master_seed=41)
+    _, Xv, Yv = S.generate(2048, 10_000, master_seed=42)
+    ens = S.Ensemble(members=4, batch=4096, seed=1)
+    hist = ens.train(X, Y, epochs=30, lr=2e-3)
+    return S, ens, hist, (Xv, Yv)
+
+
+def test_training_reduces_the_loss_and_generalises(trained):
+    S, ens, hist, (Xv, Yv) = trained
+    assert hist[-1] < 0.2 * hist[0], hist
+    pred = ens.predict(Xv)
+    ynorm = (Yv - ens.norm.y_mean) / ens.norm.y_std
+    pnorm = (pred - ens.norm.y_mean) / ens.norm.y_std
+    mse = float(((pnorm - ynorm) ** 2).mean())
+    assert mse < 0.15, mse  # held-out error well below the variance of the targets (1.0)
+
+
+def test_gate_flags_disagreement_out_of_distribution(trained):
+    S, ens, _, (Xv, _) = trained
+    inside = S.gate(ens.predict_members(Xv)).mean()
+    far = Xv.copy()
+    far[:, 0] += 3.0  # mu_a 1000x beyond the training range
+    outside = S.gate(ens.predict_members(far)).mean()
+    assert outside > inside
+
+
+def test_inverse_fit_recovers_parameters_through_the_surrogate(trained):
+    S, ens, _, (Xv, _) = trained
+    two = Xv[(Xv[:, 7] > 0) & (Xv[:, 11] == 0)][:64].copy()  # two-layer configurations
+    assert len(two) >= 16
+    obs = ens.predict(two)[:, :S.N_RD]  # noise-free, self-consistent observations
+    mask = (obs > -3.5).astype(float)
+    start = two.copy()
+    free = [0, 1, 4, 5]  # log10 mu_a, log10 mu_s' of both layers
+    start[:, free] += np.random.default_rng(3).normal(0, 0.15, (len(two), 4))
+    fit, res = S.lm_fit(ens, start, obs, mask, free, iters=40)
+    err_before = np.abs(start[:, free] - two[:, free]).mean()
+    err_after = np.abs(fit[:, free] - two[:, free]).mean()
+    assert err_after < 0.5 * err_before, (err_before, err_after)
+
+
+def test_surrogate_beats_monte_carlo_at_equal_cost(trained):
+    """What the network gains: served in batches, one surrogate query costs less GPU time than
+    tracing even 1,000 photons, and its R_d(r) (trained on 1e4-photon solves) is closer to a
+    1e5-photon solve than a 1,000-photon Monte Carlo run is."""
+    S, ens, _, _ = trained
+    cfgs, X, _ = S.generate(512, 100_000, master_seed=43)  # reference solves
+    n_q = 65536
+    Xq = np.tile(X, (n_q // len(X), 1))
+    ens.predict(Xq[:4096])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pred_q = ens.predict(Xq)
+    t_sur = (time.perf_counter() - t0) / n_q
+    cheap = (tmc.CSweepConfig * len(cfgs))(*cfgs)
+    for c in cheap:
+        c.photons = 1000
+    mc = tmc.sweep_run(cheap, tmc.sweep_options())
+    t_mc = mc.seconds / len(cfgs)
+    ref = tmc.sweep_run((tmc.CSweepConfig * len(cfgs))(*cfgs), tmc.sweep_options())
+    Yref = S.targets(ref.summary)
+    inner = slice(0, 16)
+    pred = pred_q[: len(X)]
+    err_sur = np.abs(pred[:, inner] - Yref[:, inner]).mean()
+    err_mc = np.abs(S.targets(mc.summary)[:, inner] - Yref[:, inner]).mean()
+    print(f"surrogate {t_sur * 1e6:.2f} us/query, err {err_sur:.4f}; MC(1e3 photons) {t_mc * 1e6:.2f} us/solve, "
+          f"err {err_mc:.4f}")
+    assert err_sur < err_mc, (err_sur, err_mc)
+    assert t_sur < t_mc, (t_sur, t_mc)

@@ -153,6 +153,20 @@ PROTOTYPES = {
                                                _P(CStatus)]),
     "tmc_b200_sweep_autotune": (ctypes.c_int, [_P(CSweepConfig), ctypes.c_int32, _P(CSweepOptions), _pd,
                                                _P(CStatus)]),
+    "tmc_b200_gemm_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                                          _P(CStatus)]),
+    "tmc_b200_nn_linear": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.c_int32] * 4 + [ctypes.c_void_p, _P(CStatus)]),
+    "tmc_b200_nn_backward_data": (ctypes.c_int, [ctypes.c_void_p] * 4 + [ctypes.c_int32] * 3 +
+                                  [ctypes.c_void_p, _P(CStatus)]),
+    "tmc_b200_nn_matmul_f32": (ctypes.c_int, [ctypes.c_void_p] * 3 + [ctypes.c_int32] * 3 + [ctypes.c_void_p, _P(CStatus)]),
+    "tmc_b200_nn_transpose": (ctypes.c_int, [ctypes.c_void_p] * 2 + [ctypes.c_int32] * 2 + [ctypes.c_void_p, _P(CStatus)]),
+    "tmc_b200_nn_colsum": (ctypes.c_int, [ctypes.c_void_p] * 2 + [ctypes.c_int32] * 2 + [ctypes.c_void_p, _P(CStatus)]),
+    "tmc_b200_nn_mse": (ctypes.c_int, [ctypes.c_void_p] * 4 + [ctypes.c_int32] * 3 + [ctypes.c_float, ctypes.c_void_p,
+                                                                                        _P(CStatus)]),
+    "tmc_b200_nn_adam": (ctypes.c_int, [ctypes.c_void_p] * 4 + [ctypes.c_int32] * 2 + [ctypes.c_float] * 5 +
+                         [ctypes.c_void_p] * 3 + [_P(CStatus)]),
+    "tmc_b200_nn_status": (ctypes.c_int, [ctypes.c_int32]),
     "tmc_b200_plan": (ctypes.c_int, [_P(CRunSpec), _P(COptions), ctypes.c_int32, ctypes.c_int64,
                                      ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _P(CPlan),
                                      _P(CStatus)]),
@@ -524,3 +538,20 @@ def sweep_autotune(cfgs, opt: CSweepOptions | None = None) -> tuple[CSweepOption
     st = CStatus()
     _check(lib().tmc_b200_sweep_autotune(cfgs, len(cfgs), ctypes.byref(opt), ctypes.byref(best), ctypes.byref(st)), st)
     return opt, best.value
+
+
+def gemm_bf16(A, B, bias=None, out=None):
+    """D = A @ B.T (+ bias) on the tcgen05 tensor cores for torch CUDA tensors (A: M x K bf16,
+    B: N x K bf16, K a multiple of 64); returns a float32 tensor."""
+    import torch
+
+    M, K = A.shape
+    N = B.shape[0]
+    assert A.dtype == torch.bfloat16 and B.dtype == torch.bfloat16 and B.shape[1] == K
+    A, B = A.contiguous(), B.contiguous()
+    D = out if out is not None else torch.empty((M, N), dtype=torch.float32, device=A.device)
+    st = CStatus()
+    rc = lib().tmc_b200_gemm_bf16(A.data_ptr(), B.data_ptr(), bias.data_ptr() if bias is not None else None,
+                                  D.data_ptr(), M, N, K, torch.cuda.current_stream().cuda_stream, ctypes.byref(st))
+    _check(rc, st)
+    return D

@@ -1,0 +1,352 @@
+// The surrogate's neural-network kernels and their C ABI (no counterpart in the reference: the
+// learned surrogate is an addition of this engine). Every matrix product runs on the tcgen05
+// tensor cores through gemm_tc.cuh (BF16 operands, FP32 accumulation in tensor memory) with the
+// bias, GELU and GELU-derivative work fused into its epilogue; the element-wise kernels (transpose,
+// bias gradient, loss, Adam) are plain CUDA. Entry points take device pointers and a stream and
+// do not synchronise (so a training step can be captured in a CUDA graph); a bounded tensor-core
+// wait that gives up sets a per-device status word read by tmc_b200_nn_status.
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/tissuemc_b200.h"
+#include "gemm_tc.cuh"
+
+namespace tmc {
+namespace {
+
+constexpr int kBN = 128;
+constexpr int kGemmSmemRequest = 60 * 1024;  // at most three CTAs per SM: 3 x 128 of 512 TMEM columns
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+    return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+
+// D (float32) = acc (+ bias)
+struct EpiF32 {
+    float *D;
+    const float *bias;
+    int N;
+    __device__ __forceinline__ void operator()(int row, int col, const float (&v)[8]) const {
+        float *d = D + static_cast<size_t>(row) * N + col;
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if (col + i < N) d[i] = v[i] + (bias ? bias[col + i] : 0.0f);
+    }
+};
+
+// Forward linear layer: z = acc + bias (stored as float32 if Z), h = act(z) (stored as bf16 if H).
+struct EpiFwd {
+    const float *bias;
+    float *Z;
+    __nv_bfloat16 *H;
+    int N, act;
+    __device__ __forceinline__ void operator()(int row, int col, const float (&v)[8]) const {
+        const size_t o = static_cast<size_t>(row) * N + col;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if (col + i >= N) break;
+            const float z = v[i] + bias[col + i];
+            if (Z) Z[o + i] = z;
+            if (H) H[o + i] = __float2bfloat16_rn(act ? gelu(z) : z);
+        }
+    }
+};
+
+// Backward through a linear layer into the previous GELU: dx = acc * gelu'(z_prev), bf16.
+struct EpiBwd {
+    const float *Zprev;
+    __nv_bfloat16 *dX;
+    int N;
+    __device__ __forceinline__ void operator()(int row, int col, const float (&v)[8]) const {
+        const size_t o = static_cast<size_t>(row) * N + col;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if (col + i >= N) break;
+            dX[o + i] = __float2bfloat16_rn(v[i] * gelu_grad(Zprev[o + i]));
+        }
+    }
+};
+
+__global__ void transpose_bf16_kernel(const __nv_bfloat16 *__restrict__ X, __nv_bfloat16 *__restrict__ Y, int rows,
+                                      int cols) {
+    __shared__ __nv_bfloat16 tile[32][33];
+    const int c = blockIdx.x * 32 + threadIdx.x, r0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y)
+        if (r0 + j < rows && c < cols) tile[j][threadIdx.x] = X[static_cast<size_t>(r0 + j) * cols + c];
+    __syncthreads();
+    const int r = blockIdx.y * 32 + threadIdx.x, c0 = blockIdx.x * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y)
+        if (c0 + j < cols && r < rows) Y[static_cast<size_t>(c0 + j) * rows + r] = tile[threadIdx.x][j];
+}
+
+// db[n] = sum over rows of dZ[row][n] (one thread per column, rows strided over blockIdx.y).
+__global__ void colsum_kernel(const __nv_bfloat16 *__restrict__ dZ, float *__restrict__ db, int M, int N) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    float s = 0.0f;
+    for (int m = blockIdx.y; m < M; m += gridDim.y) s += __bfloat162float(dZ[static_cast<size_t>(m) * N + n]);
+    atomicAdd(&db[n], s);
+}
+
+// Mean-squared error over the first T of ld columns: loss += scale * sum (p - t)^2 and
+// dZ = 2 * scale * (p - t) (bf16; zero in the padded columns).
+__global__ void mse_kernel(const float *__restrict__ pred, const float *__restrict__ target, __nv_bfloat16 *dZ,
+                           float *loss, int M, int T, int ld, float scale) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    if (i < static_cast<size_t>(M) * ld) {
+        const int row = static_cast<int>(i / ld), col = static_cast<int>(i % ld);
+        float g = 0.0f;
+        if (col < T) {
+            const float d = pred[i] - target[static_cast<size_t>(row) * T + col];
+            l = d * d;
+            g = 2.0f * scale * d;
+        }
+        if (dZ) dZ[i] = __float2bfloat16_rn(g);
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0 && l != 0.0f) atomicAdd(loss, l * scale);
+}
+
+// Adam on float32 master weights (rows x cols, row-major), writing the bf16 copy and its transpose.
+__global__ void adam_kernel(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
+                            float *__restrict__ v, int rows, int cols, float lr_t, float b1, float b2, float eps,
+                            float weight_decay, __nv_bfloat16 *wb, __nv_bfloat16 *wt) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= static_cast<size_t>(rows) * cols) return;
+    const float gi = g[i] + weight_decay * w[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr_t * mi / (sqrtf(vi) + eps);
+    w[i] = wi;
+    const __nv_bfloat16 b = __float2bfloat16_rn(wi);
+    if (wb) wb[i] = b;
+    if (wt) {
+        const int r = static_cast<int>(i / cols), c = static_cast<int>(i % cols);
+        wt[static_cast<size_t>(c) * rows + r] = b;
+    }
+}
+
+std::mutex g_mu;
+int *g_status[64] = {};
+bool g_attr[64] = {};
+
+void put(tmc_status *st, int code, const std::string &m) {
+    if (!st) return;
+    st->code = code;
+    std::snprintf(st->message, sizeof st->message, "%s", m.c_str());
+}
+
+int current_device() {
+    int d = -1;
+    if (cudaGetDevice(&d) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return d;
+}
+
+// The per-device status word (allocated at the first call on a device, before any capture).
+int *status_word(int dev) {
+    if (dev < 0 || dev >= 64) return nullptr;
+    if (!g_status[dev]) {
+        if (cudaMalloc(&g_status[dev], sizeof(int)) != cudaSuccess) return nullptr;
+        if (cudaMemset(g_status[dev], 0, sizeof(int)) != cudaSuccess) return nullptr;
+    }
+    return g_status[dev];
+}
+
+template <class Epi> void set_smem_attr() {
+    cudaFuncSetAttribute(gemm_tc_kernel<kBN, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmemRequest);
+}
+
+// Common checks and the launch of one tensor-core GEMM (asynchronous).
+template <class Epi>
+int launch_gemm(const void *A, const void *B, int M, int N, int K, const Epi &epi, void *stream, tmc_status *st) {
+    if (!A || !B) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument");
+        return TMC_BAD_ARGUMENT;
+    }
+    if (M < 1 || N < 1 || K < 64 || K % 64 != 0) {
+        put(st, TMC_BAD_CONFIG, "tensor-core GEMM needs M, N >= 1 and K a positive multiple of 64");
+        return TMC_BAD_CONFIG;
+    }
+    const int dev = current_device();
+    std::lock_guard<std::mutex> lock(g_mu);
+    int *status = status_word(dev);
+    if (!status) {
+        put(st, TMC_NO_DEVICE, "no usable CUDA device found");
+        return TMC_NO_DEVICE;
+    }
+    if (!g_attr[dev]) {
+        set_smem_attr<EpiF32>();
+        set_smem_attr<EpiFwd>();
+        set_smem_attr<EpiBwd>();
+        g_attr[dev] = true;
+    }
+    const dim3 grid((N + kBN - 1) / kBN, (M + kGemmBM - 1) / kGemmBM);
+    gemm_tc_kernel<kBN, Epi><<<grid, kGemmThreads, kGemmSmemRequest, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16 *>(A), static_cast<const __nv_bfloat16 *>(B), M, N, K, epi, status);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        put(st, TMC_CUDA_ERROR, std::string("CUDA error launching the tensor-core GEMM: ") + cudaGetErrorString(e));
+        return TMC_CUDA_ERROR;
+    }
+    return TMC_OK;
+}
+
+int launched(tmc_status *st) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        put(st, TMC_CUDA_ERROR, std::string("CUDA error: ") + cudaGetErrorString(e));
+        return TMC_CUDA_ERROR;
+    }
+    return TMC_OK;
+}
+
+}  // namespace
+}  // namespace tmc
+
+using namespace tmc;
+
+extern "C" {
+
+int tmc_b200_gemm_bf16(const uint16_t *A, const uint16_t *B, const float *bias, float *D, int32_t M, int32_t N,
+                       int32_t K, void *stream, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!D) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument");
+        return TMC_BAD_ARGUMENT;
+    }
+    const int dev = current_device();
+    int *status = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        status = status_word(dev);
+    }
+    if (!status) {
+        put(st, TMC_NO_DEVICE, "no usable CUDA device found");
+        return TMC_NO_DEVICE;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaMemsetAsync(status, 0, sizeof(int), s);
+    const int rc = launch_gemm(A, B, M, N, K, EpiF32{D, bias, N}, stream, st);
+    if (rc != TMC_OK) return rc;
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        put(st, TMC_CUDA_ERROR, std::string("CUDA error in the tensor-core GEMM: ") + cudaGetErrorString(e));
+        return TMC_CUDA_ERROR;
+    }
+    int h = 0;
+    cudaMemcpy(&h, status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (h) {
+        put(st, TMC_DEVICE_TIMEOUT, "a tensor-core wait gave up (mbarrier poll limit)");
+        return TMC_DEVICE_TIMEOUT;
+    }
+    return TMC_OK;
+}
+
+int tmc_b200_nn_linear(const uint16_t *X, const uint16_t *W, const float *bias, float *Z, uint16_t *H, int32_t M,
+                       int32_t N, int32_t K, int32_t gelu_act, void *stream, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!bias || (!Z && !H)) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument");
+        return TMC_BAD_ARGUMENT;
+    }
+    return launch_gemm(X, W, M, N, K, EpiFwd{bias, Z, reinterpret_cast<__nv_bfloat16 *>(H), N, gelu_act}, stream, st);
+}
+
+int tmc_b200_nn_backward_data(const uint16_t *dZ, const uint16_t *WT, const float *Zprev, uint16_t *dX, int32_t M,
+                              int32_t N, int32_t K, void *stream, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!Zprev || !dX) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument");
+        return TMC_BAD_ARGUMENT;
+    }
+    return launch_gemm(dZ, WT, M, N, K, EpiBwd{Zprev, reinterpret_cast<__nv_bfloat16 *>(dX), N}, stream, st);
+}
+
+int tmc_b200_nn_matmul_f32(const uint16_t *A, const uint16_t *B, float *D, int32_t M, int32_t N, int32_t K,
+                           void *stream, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!D) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument");
+        return TMC_BAD_ARGUMENT;
+    }
+    return launch_gemm(A, B, M, N, K, EpiF32{D, nullptr, N}, stream, st);
+}
+
+int tmc_b200_nn_transpose(const uint16_t *X, uint16_t *Y, int32_t rows, int32_t cols, void *stream,
+                          tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!X || !Y || rows < 1 || cols < 1) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument or empty matrix");
+        return TMC_BAD_ARGUMENT;
+    }
+    transpose_bf16_kernel<<<dim3((cols + 31) / 32, (rows + 31) / 32), dim3(32, 8), 0,
+                            static_cast<cudaStream_t>(stream)>>>(reinterpret_cast<const __nv_bfloat16 *>(X),
+                                                                 reinterpret_cast<__nv_bfloat16 *>(Y), rows, cols);
+    return launched(st);
+}
+
+int tmc_b200_nn_colsum(const uint16_t *dZ, float *db, int32_t M, int32_t N, void *stream, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!dZ || !db || M < 1 || N < 1) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument or empty matrix");
+        return TMC_BAD_ARGUMENT;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaMemsetAsync(db, 0, sizeof(float) * N, s);
+    colsum_kernel<<<dim3((N + 127) / 128, 64), 128, 0, s>>>(reinterpret_cast<const __nv_bfloat16 *>(dZ), db, M, N);
+    return launched(st);
+}
+
+int tmc_b200_nn_mse(const float *pred, const float *target, uint16_t *dZ, float *loss, int32_t M, int32_t T,
+                    int32_t ld, float scale, void *stream, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!pred || !target || !loss || M < 1 || T < 1 || ld < T) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument or bad shape");
+        return TMC_BAD_ARGUMENT;
+    }
+    const size_t n = static_cast<size_t>(M) * ld;
+    mse_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        pred, target, reinterpret_cast<__nv_bfloat16 *>(dZ), loss, M, T, ld, scale);
+    return launched(st);
+}
+
+int tmc_b200_nn_adam(float *w, const float *g, float *m, float *v, int32_t rows, int32_t cols, float lr_t, float b1,
+                     float b2, float eps, float weight_decay, uint16_t *wb, uint16_t *wt, void *stream,
+                     tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!w || !g || !m || !v || rows < 1 || cols < 1) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument or empty parameter");
+        return TMC_BAD_ARGUMENT;
+    }
+    const size_t n = static_cast<size_t>(rows) * cols;
+    adam_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        w, g, m, v, rows, cols, lr_t, b1, b2, eps, weight_decay, reinterpret_cast<__nv_bfloat16 *>(wb),
+        reinterpret_cast<__nv_bfloat16 *>(wt));
+    return launched(st);
+}
+
+int tmc_b200_nn_status(int32_t clear) {
+    const int dev = current_device();
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (dev < 0 || dev >= 64 || !g_status[dev]) return 0;
+    int h = 0;
+    cudaMemcpy(&h, g_status[dev], sizeof(int), cudaMemcpyDeviceToHost);
+    if (clear) cudaMemset(g_status[dev], 0, sizeof(int));
+    return h;
+}
+
+}  // extern "C"

@@ -104,9 +104,10 @@ template <int FAST> struct SweepCtx {
     }
 };
 
-// Minimum resident 256-thread blocks per SM the compiler must allow for (0: no bound).
+// Minimum resident 256-thread blocks per SM the compiler must allow for (0: no bound); 4 caps the
+// sweep kernel at 64 registers, measured 2.3 % faster than its unbounded 73 registers.
 #ifndef TMC_SWEEP_MIN_BLOCKS
-#define TMC_SWEEP_MIN_BLOCKS 0
+#define TMC_SWEEP_MIN_BLOCKS 4
 #endif
 #if TMC_SWEEP_MIN_BLOCKS > 0
 #define TMC_SWEEP_BOUNDS __launch_bounds__(256, TMC_SWEEP_MIN_BLOCKS)
