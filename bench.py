@@ -38,6 +38,7 @@ WORKLOADS = {
     "skin5": "five-layer skin stack (n=1.4 in air; 1e8 photons; dr=0.002 cm x 500, dz=0.001 cm x 400, na=30)",
     "slab_n14": "single slab n=1.4 in air (mua=5, mus=95, g=0.8, d=0.05 cm; 1e6 photons; 50x20 grid, na=30)",
     "sweep": SWEEP_DESC,
+    "surrogate": "learned surrogate trained on sweep solves; gated serving and inverse fits",
 }
 METRIC = "photons/s on 1 B200 (plain MC)"
 
@@ -63,6 +64,8 @@ def _args():
     ap.add_argument("--photons", type=int, default=0,
                     help="override the workload's photon count (for profiling captures only)")
     ap.add_argument("--autotune", action="store_true", help="sweep: pick the launch shape first")
+    ap.add_argument("--scale", type=float, default=1.0, help="surrogate: fraction of the full data and query counts")
+    ap.add_argument("--epochs", type=int, default=20, help="surrogate: training epochs")
     ap.add_argument("--no-profiles", action="store_true",
                     help="diagnostic: skip the profile tallies (rung 6 without profiles); not a result")
     return ap.parse_args()
@@ -234,10 +237,30 @@ def run_sweep(a) -> None:
         }), flush=True)
 
 
+def run_surrogate(a) -> None:
+    """The learned surrogate end to end (training data from the batched sweep, training, accuracy
+    against high-photon MC, gated serving, inverse fits); one JSON line of its measurements."""
+    from tissuemc_b200 import surrogate
+
+    rank, world, local = _dist()
+    res = surrogate.pipeline(scale=a.scale, epochs=a.epochs, log=lambda m: print(m, file=sys.stderr, flush=True))
+    if rank == 0:
+        s = res["serving"]
+        print(json.dumps({
+            "metric": "gated surrogate queries/s on 1 B200", "value": s["gated_queries_per_s"], "unit": "queries/s",
+            "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 GEMMs, fp32 accumulation", "data": "synthetic (sweep-generated)",
+            "config": {"workload": "surrogate: 12+1 -> 4x512 GELU -> 66 MLP, 4 members, batch 4096", "scale": a.scale},
+            "speedup_vs_plain_mc": s["speedup_vs_plain_mc"], "details": res}), flush=True)
+
+
 def main() -> None:
     a = _args()
     if a.impl == "reference":
         run_reference_arm(a)
+        return
+    if a.workload == "surrogate":
+        run_surrogate(a)
         return
     if a.workload == "sweep":
         run_sweep(a)

@@ -307,6 +307,19 @@ TMC_B200_API int tmc_b200_nn_adam(float *w, const float *g, float *m, float *v, 
                                   float lr_t, float b1, float b2, float eps, float weight_decay, uint16_t *wb,
                                   uint16_t *wt, void *stream, tmc_status *status);
 TMC_B200_API int tmc_b200_nn_status(int32_t clear);
+/* encode: X (n x ld, bf16) = z-scored feats (n x nf, float32), zero-padded to ld columns.
+ * gate:   per query, each member's diffuse reflectance on the grid from its normalised outputs
+ *         Z[m] (n x ld float32, members member_stride elements apart), de-normalised with ymean,
+ *         ystd (log10 R_d(r) per area in the first nbins columns) and weighted by the annulus
+ *         areas; rd_mean (optional) gets the members' mean, spread (optional) their sample standard
+ *         deviation over the mean, and route[q] = 1 when the spread exceeds threshold (the query
+ *         goes to Monte Carlo). */
+TMC_B200_API int tmc_b200_nn_encode(const float *feats, const float *mean, const float *stdv, uint16_t *X, int32_t n,
+                                    int32_t nf, int32_t ld, void *stream, tmc_status *status);
+TMC_B200_API int tmc_b200_nn_gate(const float *Z, int32_t members, int64_t member_stride, int32_t ld,
+                                  const float *ymean, const float *ystd, const float *areas, int32_t nbins, int32_t n,
+                                  float threshold, float *rd_mean, float *spread, uint8_t *route, void *stream,
+                                  tmc_status *status);
 
 /* Parse an MCML .mci file (the reference's parse_mci_file, src/io/mci.cpp:173-183): writes up to
  * `max_runs` runs and returns the number found in *n_runs. Errors carry the line number. */

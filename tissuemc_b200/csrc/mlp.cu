@@ -137,6 +137,42 @@ __global__ void adam_kernel(float *__restrict__ w, const float *__restrict__ g, 
     }
 }
 
+// Network inputs from raw features: z-score the first nf of n_feat columns, zero-pad to ld, bf16.
+__global__ void encode_kernel(const float *__restrict__ feats, const float *__restrict__ mean,
+                              const float *__restrict__ stdv, __nv_bfloat16 *__restrict__ X, int n, int nf, int ld) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= static_cast<size_t>(n) * ld) return;
+    const int row = static_cast<int>(i / ld), col = static_cast<int>(i % ld);
+    const float v = col < nf ? (feats[static_cast<size_t>(row) * nf + col] - mean[col]) / stdv[col] : 0.0f;
+    X[i] = __float2bfloat16_rn(v);
+}
+
+// The ensemble gate: for each query, every member's diffuse reflectance on the grid
+// (sum over bins of 10^(z * std + mean) * area), their mean, their spread (sample standard
+// deviation over the mean) and whether the spread exceeds the threshold (route the query to Monte
+// Carlo).
+__global__ void gate_kernel(const float *__restrict__ Z, int members, size_t member_stride, int ld,
+                            const float *__restrict__ ymean, const float *__restrict__ ystd,
+                            const float *__restrict__ areas, int nbins, int n, float threshold, float *rd_mean,
+                            float *spread, unsigned char *route) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    float s1 = 0.0f, s2 = 0.0f;
+    for (int m = 0; m < members; ++m) {
+        const float *z = Z + m * member_stride + static_cast<size_t>(q) * ld;
+        float rd = 0.0f;
+        for (int b = 0; b < nbins; ++b) rd += exp10f(z[b] * ystd[b] + ymean[b]) * areas[b];
+        s1 += rd;
+        s2 += rd * rd;
+    }
+    const float mean = s1 / members;
+    const float var = members > 1 ? fmaxf(s2 - s1 * mean, 0.0f) / (members - 1) : 0.0f;
+    const float sp = sqrtf(var) / fmaxf(mean, 1e-12f);
+    if (rd_mean) rd_mean[q] = mean;
+    if (spread) spread[q] = sp;
+    route[q] = sp > threshold ? 1 : 0;
+}
+
 std::mutex g_mu;
 int *g_status[64] = {};
 bool g_attr[64] = {};
@@ -336,6 +372,33 @@ int tmc_b200_nn_adam(float *w, const float *g, float *m, float *v, int32_t rows,
     adam_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         w, g, m, v, rows, cols, lr_t, b1, b2, eps, weight_decay, reinterpret_cast<__nv_bfloat16 *>(wb),
         reinterpret_cast<__nv_bfloat16 *>(wt));
+    return launched(st);
+}
+
+int tmc_b200_nn_encode(const float *feats, const float *mean, const float *stdv, uint16_t *X, int32_t n, int32_t nf,
+                       int32_t ld, void *stream, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!feats || !mean || !stdv || !X || n < 1 || nf < 1 || ld < nf) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument or bad shape");
+        return TMC_BAD_ARGUMENT;
+    }
+    const size_t total = static_cast<size_t>(n) * ld;
+    encode_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        feats, mean, stdv, reinterpret_cast<__nv_bfloat16 *>(X), n, nf, ld);
+    return launched(st);
+}
+
+int tmc_b200_nn_gate(const float *Z, int32_t members, int64_t member_stride, int32_t ld, const float *ymean,
+                     const float *ystd, const float *areas, int32_t nbins, int32_t n, float threshold, float *rd_mean,
+                     float *spread, uint8_t *route, void *stream, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!Z || !ymean || !ystd || !areas || !route || members < 1 || n < 1 || nbins < 1 || ld < nbins) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument or bad shape");
+        return TMC_BAD_ARGUMENT;
+    }
+    gate_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        Z, members, static_cast<size_t>(member_stride), ld, ymean, ystd, areas, nbins, n, threshold, rd_mean, spread,
+        route);
     return launched(st);
 }
 

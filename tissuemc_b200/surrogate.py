@@ -32,14 +32,29 @@ LAYER_DIMS = [(K_IN, HIDDEN)] + [(HIDDEN, HIDDEN)] * (N_HIDDEN - 1) + [(HIDDEN, 
 
 
 # ------------------------------------------------------------------------------ encoding
+_CFG_DTYPE = np.dtype([("photons", "<u8"), ("seed", "<u8"), ("n_above", "<f8"), ("n_below", "<f8"),
+                       ("num_layers", "<i4"), ("pad", "<i4"), ("layers", "<f8", (16, 5))])
+
+
 def features(cfgs) -> np.ndarray:
-    """(n, 13) raw features of sweep configurations (see the module docstring)."""
-    out = np.zeros((len(cfgs), N_FEAT))
-    for i, c in enumerate(cfgs):
-        for l in range(min(c.num_layers, 3)):
-            L = c.layers[l]
-            out[i, 4 * l:4 * l + 4] = (math.log10(L.mua), math.log10(L.mus * (1.0 - L.g)), L.g, L.d)
-        out[i, 12] = c.layers[0].n
+    """(n, 13) raw features of sweep configurations (see the module docstring), vectorised over
+    the ctypes array's memory."""
+    import ctypes as _ct
+
+    assert _CFG_DTYPE.itemsize == _ct.sizeof(CSweepConfig)
+    if isinstance(cfgs, _ct.Array):
+        a = np.frombuffer(cfgs, dtype=_CFG_DTYPE, count=len(cfgs))
+    else:
+        a = np.frombuffer(b"".join(bytes(c) for c in cfgs), dtype=_CFG_DTYPE)
+    lay = a["layers"][:, :3, :]  # n, mua, mus, g, d
+    present = np.arange(3)[None, :] < a["num_layers"][:, None]
+    out = np.zeros((len(a), N_FEAT))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        block = np.stack([np.log10(lay[..., 1]), np.log10(lay[..., 2] * (1.0 - lay[..., 3])), lay[..., 3],
+                          lay[..., 4]], axis=-1)
+    block[~present] = 0.0
+    out[:, :12] = block.reshape(len(a), 12)
+    out[:, 12] = lay[:, 0, 0]
     return out
 
 
@@ -267,11 +282,71 @@ def rd_total(y_raw: np.ndarray, dr: float = 0.01) -> np.ndarray:
     return (rd_profile(y_raw) * annulus_areas(N_RD, dr)).sum(-1)
 
 
-def gate(members_out: np.ndarray, threshold: float = 0.01) -> np.ndarray:
-    """True where the members disagree: relative spread (max - min) / mean of the predicted
-    diffuse reflectance above `threshold` — those queries go back to plain Monte Carlo."""
+class Server:
+    """Gated serving on the device: encode, every member's forward pass and the gate run in this
+    package's kernels on one stream; the host sends raw features and receives the ensemble mean
+    outputs, the members' mean R_d on the grid and the routing flags."""
+
+    def __init__(self, ens: Ensemble, chunk: int = 65536, threshold: float = 0.01):
+        import torch
+
+        t = self.torch = torch
+        self.ens, self.chunk, self.threshold = ens, chunk, threshold
+        dev = ens.dev
+        nm = ens.norm
+        self.x_mean = t.tensor(nm.x_mean, dtype=t.float32, device=dev)
+        self.x_std = t.tensor(nm.x_std, dtype=t.float32, device=dev)
+        self.y_mean = t.tensor(nm.y_mean, dtype=t.float32, device=dev)
+        self.y_std = t.tensor(nm.y_std, dtype=t.float32, device=dev)
+        self.areas = t.tensor(annulus_areas(), dtype=t.float32, device=dev)
+        M = len(ens.members)
+        self.feats = t.empty(chunk, N_FEAT, dtype=t.float32, device=dev)
+        self.X = t.empty(chunk, K_IN, dtype=t.bfloat16, device=dev)
+        self.Z = t.empty(M, chunk, N_OUT_PAD, dtype=t.float32, device=dev)
+        self.rd = t.empty(chunk, dtype=t.float32, device=dev)
+        self.spread = t.empty(chunk, dtype=t.float32, device=dev)
+        self.route = t.empty(chunk, dtype=t.uint8, device=dev)
+        for m in ens.members:
+            _ensure_rows(m, chunk)
+
+    def __call__(self, feats: np.ndarray, spreads: list | None = None):
+        """(mean raw outputs (n, 66), mean R_d on the grid (n,), route flags (n,)); the members'
+        spreads are appended to `spreads` when it is given."""
+        t = self.torch
+        n = len(feats)
+        s = t.cuda.current_stream().cuda_stream
+        outs, rds, routes = [], [], []
+        src = t.from_numpy(np.ascontiguousarray(feats, dtype=np.float32)).pin_memory()
+        for a in range(0, n, self.chunk):
+            rows = min(self.chunk, n - a)
+            self.feats[:rows].copy_(src[a:a + rows], non_blocking=True)
+            _call("tmc_b200_nn_encode", _p(self.feats), _p(self.x_mean), _p(self.x_std), _p(self.X), rows, N_FEAT,
+                  K_IN, ctypes.c_void_p(s))
+            for i, m in enumerate(self.ens.members):
+                m.forward(self.X, rows, s, Z_out=self.Z[i])
+            _call("tmc_b200_nn_gate", _p(self.Z), len(self.ens.members), self.chunk * N_OUT_PAD, N_OUT_PAD,
+                  _p(self.y_mean), _p(self.y_std), _p(self.areas), N_RD, rows, ctypes.c_float(self.threshold),
+                  _p(self.rd), _p(self.spread), _p(self.route), ctypes.c_void_p(s))
+            outs.append(self.Z[:, :rows, :N_OUT].mean(0).cpu())
+            rds.append(self.rd[:rows].cpu())
+            if spreads is not None:
+                spreads.append(self.spread[:rows].cpu().numpy())
+            routes.append(self.route[:rows].cpu())
+        y = t.cat(outs).numpy() * self.ens.norm.y_std + self.ens.norm.y_mean
+        return y, t.cat(rds).numpy(), t.cat(routes).numpy().astype(bool)
+
+
+def spread(members_out: np.ndarray) -> np.ndarray:
+    """The members' disagreement on the predicted diffuse reflectance: sample standard deviation
+    over the mean of each member's R_d on the grid."""
     rd = rd_total(members_out)
-    return (rd.max(0) - rd.min(0)) / np.maximum(rd.mean(0), 1e-12) > threshold
+    return rd.std(0, ddof=1) / np.maximum(rd.mean(0), 1e-12)
+
+
+def gate(members_out: np.ndarray, threshold: float = 0.01) -> np.ndarray:
+    """True where the members disagree by more than `threshold` — those queries go back to plain
+    Monte Carlo."""
+    return spread(members_out) > threshold
 
 
 # ------------------------------------------------------------------------------ inverse fit
@@ -329,3 +404,141 @@ def config_from_features(f: np.ndarray, photons: int, seed: int) -> CSweepConfig
         nl += 1
     c.num_layers = nl
     return c
+
+
+# ------------------------------------------------------------------------------ the pipeline
+def pipeline(scale: float = 1.0, members: int = 4, epochs: int = 20, seed: int = 0, log=print) -> dict:
+    """Train, evaluate and serve the surrogate end to end; returns the measurements.
+
+    Full size (scale 1): 2^20 training and 2^16 held-out solves at 1e5 photons from the batched
+    sweep; accuracy on 64 held-out configurations against 1e8-photon Monte Carlo (bins with at
+    least 1e4 photons' worth of signal, i.e. R_d(r) * area * 1e8 >= 1e4); 1e6 gated queries in
+    batches of 65,536 (queries whose members' R_d disagree by more than 1 % go back to plain Monte
+    Carlo at 1e6 photons, one batched sweep); 1024 inverse fits of (mu_a, mu_s') of both layers of
+    two-layer tissues from noisy 1e6-photon R_d(r), each verified by a plain-MC solve at the fit.
+    `scale` shrinks the counts (not the network) for quick runs."""
+    import time
+
+    import torch
+
+    from . import sweep_sample
+
+    out: dict = {"scale": scale, "members": members, "epochs": epochs}
+    n_train, n_hold = max(4096, int(2 ** 20 * scale)), max(1024, int(2 ** 16 * scale))
+    n_train -= n_train % 4096
+    photons = 100_000 if scale >= 0.05 else 10_000
+    t0 = time.perf_counter()
+    _, X, Y = generate(n_train, photons, master_seed=1000 + seed)
+    hcfg, Xh, Yh = generate(n_hold, photons, master_seed=2000 + seed)
+    torch.cuda.synchronize()
+    out["data"] = {"train_solves": n_train, "held_out_solves": n_hold, "photons_per_solve": photons,
+                   "seconds": time.perf_counter() - t0}
+    log(f"data: {out['data']}")
+
+    t0 = time.perf_counter()
+    ens = Ensemble(members=members, batch=4096, seed=seed)
+    hist = ens.train(X, Y, epochs=epochs, lr=2e-3)
+    torch.cuda.synchronize()
+    out["train"] = {"seconds": time.perf_counter() - t0, "loss_first": hist[0], "loss_last": hist[-1]}
+    ph = ens.predict(Xh)
+    out["held_out_mse_normalised"] = float((((ph - Yh) / ens.norm.y_std) ** 2).mean())
+    log(f"train: {out['train']}, held-out normalised MSE {out['held_out_mse_normalised']:.4f}")
+
+    # accuracy against high-photon Monte Carlo
+    n_acc = max(8, int(64 * min(1.0, scale * 4)))
+    acc_photons = 100_000_000 if scale >= 0.25 else 10_000_000
+    acc_cfgs = (CSweepConfig * n_acc)(*hcfg[:n_acc])
+    for c in acc_cfgs:
+        c.photons = acc_photons
+    ref = sweep_run(acc_cfgs, sweep_options()).summary
+    areas = annulus_areas()
+    ref_rd = ref[:, :N_RD] / areas
+    pred_rd = rd_profile(ens.predict(Xh[:n_acc]))
+    counted = ref[:, :N_RD] * acc_photons >= 1e4  # bins with at least ~1e4 photons of signal
+    rel = np.abs(pred_rd - ref_rd) / np.maximum(ref_rd, 1e-30)
+    out["accuracy_vs_mc"] = {"configs": n_acc, "mc_photons": acc_photons, "bins": int(counted.sum()),
+                             "median_rel_err": float(np.median(rel[counted])),
+                             "p90_rel_err": float(np.quantile(rel[counted], 0.9)),
+                             "frac_bins_within_1pct": float((rel[counted] <= 0.01).mean())}
+    log(f"accuracy: {out['accuracy_vs_mc']}")
+
+    # gated serving
+    n_q = max(65536, int(1_000_000 * scale))
+    qcfg = sweep_sample(3000 + seed, n_q)
+    Xq = features(qcfg)
+    server = Server(ens)
+    server(Xq[:65536])  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    spreads: list = []
+    _, _, routed = server(Xq, spreads)
+    torch.cuda.synchronize()
+    t_net = time.perf_counter() - t0
+    sp = np.concatenate(spreads)
+    out["routing_vs_threshold"] = {f"{th:g}": float((sp > th).mean()) for th in (0.005, 0.01, 0.02, 0.05)}
+    # error of the surrogate on the accuracy subset, split by what the gate decides
+    sp_acc = spread(ens.predict_members(Xh[:n_acc]))
+    keep = sp_acc <= 0.01
+    if keep.any():
+        out["accuracy_vs_mc"]["kept_by_gate"] = int(keep.sum())
+        out["accuracy_vs_mc"]["kept_median_rel_err"] = float(np.median(rel[keep][counted[keep]]))
+        out["accuracy_vs_mc"]["kept_frac_bins_within_1pct"] = float((rel[keep][counted[keep]] <= 0.01).mean())
+    idx = np.flatnonzero(routed)
+    t_mc, simulated = 0.0, 0
+    if len(idx):
+        # the routed queries as batched sweeps at 1e6 photons; beyond 65,536 of them the time is
+        # extrapolated from the first 65,536 (the cost is linear in the count)
+        sim = idx[:65536]
+        mc_cfgs = (CSweepConfig * len(sim))(*[qcfg[i] for i in sim])
+        for c in mc_cfgs:
+            c.photons = 1_000_000
+        t1 = time.perf_counter()
+        for s in range(0, len(sim), 4096):
+            part = (CSweepConfig * min(4096, len(sim) - s))(*mc_cfgs[s:s + 4096])
+            sweep_run(part, sweep_options())
+        simulated = len(sim)
+        t_mc = (time.perf_counter() - t1) * len(idx) / len(sim)
+    # plain MC at 1e6 photons for a sample of the same queries: its solves/s
+    sample = (CSweepConfig * 4096)(*qcfg[:4096])
+    for c in sample:
+        c.photons = 1_000_000
+    mc_sample = sweep_run(sample, sweep_options())
+    mc_rate = 4096 / mc_sample.seconds
+    gated_rate = n_q / (t_net + t_mc)
+    out["serving"] = {"queries": n_q, "routed_to_mc": int(len(idx)), "routed_fraction": len(idx) / n_q,
+                      "routed_simulated": simulated,
+                      "network_seconds": t_net, "mc_seconds": t_mc, "gated_queries_per_s": gated_rate,
+                      "network_queries_per_s": n_q / t_net, "plain_mc_solves_per_s_1e6_photons": mc_rate,
+                      "speedup_vs_plain_mc": gated_rate / mc_rate}
+    log(f"serving: {out['serving']}")
+
+    # inverse fits of two-layer tissues
+    n_fit = max(64, int(1024 * scale))
+    cand = sweep_sample(4000 + seed, 8 * n_fit)
+    two = [c for c in cand if c.num_layers == 2][:n_fit]
+    truth = features(two)
+    obs_cfgs = (CSweepConfig * len(two))(*two)
+    for c in obs_cfgs:
+        c.photons = 1_000_000
+    obs = sweep_run(obs_cfgs, sweep_options()).summary
+    rng = np.random.default_rng(seed)
+    noisy = obs[:, :N_RD] * (1 + 0.02 * rng.standard_normal(obs[:, :N_RD].shape))  # 2 % measurement noise
+    obs_log = np.log10(np.maximum(noisy / areas, RD_FLOOR))
+    mask = (obs[:, :N_RD] * 1e6 >= 1e3).astype(float)
+    free = [0, 1, 4, 5]
+    start = truth.copy()
+    start[:, free] = np.array([X[:, j].mean() for j in free])  # start from the prior's centre
+    t0 = time.perf_counter()
+    fit, res = lm_fit(ens, start, obs_log, mask, free, iters=30)
+    t_fit = time.perf_counter() - t0
+    ver = (CSweepConfig * len(two))(*[config_from_features(f, 1_000_000, 77 + i) for i, f in enumerate(fit)])
+    vsum = sweep_run(ver, sweep_options()).summary
+    v_log = np.log10(np.maximum(vsum[:, :N_RD] / areas, RD_FLOOR))
+    v_rms = np.sqrt((((v_log - obs_log) * mask) ** 2).sum(1) / np.maximum(mask.sum(1), 1))
+    err = np.abs(fit[:, free] - truth[:, free])
+    out["inverse_fit"] = {"fits": len(two), "seconds": t_fit, "median_abs_log10_err": [float(np.median(err[:, j]))
+                                                                                        for j in range(4)],
+                          "verified_rms_log10_residual_median": float(np.median(v_rms)),
+                          "verified_within_5pct": float((v_rms < np.log10(1.05)).mean())}
+    log(f"inverse fit: {out['inverse_fit']}")
+    return out
