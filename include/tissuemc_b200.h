@@ -326,6 +326,13 @@ TMC_B200_API int tmc_b200_nn_gate(const float *Z, int32_t members, int64_t membe
 TMC_B200_API int tmc_b200_parse_mci(const char *path, tmc_run_spec *runs, int32_t max_runs, int32_t *n_runs,
                        tmc_status *status);
 
+/* Write a finished run as an MCML output file (.mco: InParm, RAT, A_l, A_z, Rd_r, Rd_a, Tt_r, Tt_a,
+ * A_rz, Rd_ra, Tt_ra, scaled per area, solid angle and volume as the MCML manual defines them).
+ * `result` must carry the batch totals and the optional 2-D arrays a_rz, rd_ra and tt_ra. No
+ * reference counterpart: TissueMC writes JSON only (src/io/result.cpp). Pure host code. */
+TMC_B200_API int tmc_b200_write_mco(const tmc_run_spec *spec, const tmc_options *opt, const tmc_result *result,
+                                    const char *path, tmc_status *status);
+
 #ifdef __cplusplus
 }
 #endif

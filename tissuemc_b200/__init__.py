@@ -143,6 +143,7 @@ PROTOTYPES = {
     "tmc_b200_parse_mci": (ctypes.c_int, [ctypes.c_char_p, _P(CRunSpec), ctypes.c_int32,
                                           _P(ctypes.c_int32), _P(CStatus)]),
     "tmc_b200_run_static": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _P(CResult), _P(CStatus)]),
+    "tmc_b200_write_mco": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _P(CResult), ctypes.c_char_p, _P(CStatus)]),
     "tmc_b200_sweep_default_options": (None, [_P(CSweepOptions)]),
     "tmc_b200_sweep_sample": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int32, _P(CSweepConfig), _P(CStatus)]),
     "tmc_b200_sweep_sizes": (ctypes.c_int, [_P(CSweepConfig), ctypes.c_int32, _P(CSweepOptions),
@@ -447,6 +448,27 @@ def parse_mci(path: str | Path) -> list[RunSpec]:
     if n.value > 64:
         raise ConfigError(f"{path}: more than 64 runs")
     return [RunSpec.from_c(runs[i], name=Path(path).stem + ".mco") for i in range(n.value)]
+
+
+def write_mco(result: RunResult, path: str | Path) -> None:
+    """Write a run as an MCML output file (.mco) with the engine's C++ writer; `read_mco` in
+    tissuemc_b200.mco reads it back."""
+    opt = options(seed=result.seed, batches=len(result.photons))
+    res = CResult()
+    keep = {}
+    for k in ("first_photon", "photons", "rd", "tt", "absorbed", "events", "anomalies", "a_z", "rd_r", "tt_r",
+              "a_rz", "rd_ra", "tt_ra"):
+        a = getattr(result, k)
+        a = keep[k] = np.ascontiguousarray(a, dtype=np.uint64 if a.dtype == np.uint64 else np.float64)
+        ct = ctypes.c_uint64 if a.dtype == np.uint64 else ctypes.c_double
+        setattr(res, k, a.ctypes.data_as(ctypes.POINTER(ct)))
+    res.specular = result.specular
+    res.kernel_seconds = result.kernel_seconds
+    res.device = result.device.encode()[:127]
+    st = CStatus()
+    c = result.spec.to_c()
+    _check(lib().tmc_b200_write_mco(ctypes.byref(c), ctypes.byref(opt), ctypes.byref(res), str(path).encode(),
+                                    ctypes.byref(st)), st)
 
 
 def workload(name: str) -> RunSpec:

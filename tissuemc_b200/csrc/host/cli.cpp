@@ -4,7 +4,7 @@
 //   tissuemc --version
 //   tissuemc run <input.mci> [--photons N] [--batches B] [--seed S] [--threads T] [--precision P]
 //                            [--engine cuda|b200] [--rung N] [--gpu-tally P] [--no-profiles]
-//                            [--output FILE]
+//                            [--output FILE] [--mco FILE]
 //
 // --engine defaults to the GPU here: this binary carries the B200 engine only (the reference's CPU
 // engine stays the reference's). --threads and --precision are accepted and recorded as the
@@ -17,6 +17,7 @@
 #include <fstream>
 #include <string>
 
+#include "../../../include/tissuemc_b200.h"
 #include "tissuemc_api.hpp"
 
 namespace {
@@ -37,7 +38,9 @@ void usage(std::FILE *to) {
                  "  --rung N       accepted for compatibility: 0, 1, 3, 5, 6, 7 or 8\n"
                  "  --gpu-tally P  accepted for compatibility (tallies are 64-bit fixed point)\n"
                  "  --no-profiles  diagnostic for rung 6: skip the profile tallies\n"
-                 "  --output FILE  write full results as JSON\n");
+                 "  --output FILE  write full results as JSON\n"
+                 "  --mco FILE     also write each run as an MCML output file (FILE, or FILE's stem\n"
+                 "                 with _<run> appended when the input holds several runs)\n");
 }
 
 unsigned long long count_arg(const char *name, const char *text) {
@@ -50,6 +53,55 @@ unsigned long long count_arg(const char *name, const char *text) {
     return v;
 }
 
+// The run as an MCML .mco file through the library's writer (tmc_b200_write_mco).
+bool write_mco(const tissuemc::RunSpec &spec, const tissuemc::EngineOptions &opt, const tissuemc::RunResult &res,
+               const std::string &path) {
+    tmc_run_spec c{};
+    c.photons = res.photons();
+    c.dz = spec.dz;
+    c.dr = spec.dr;
+    c.nz = spec.nz;
+    c.nr = spec.nr;
+    c.na = spec.na;
+    c.n_above = spec.n_above;
+    c.n_below = spec.n_below;
+    c.num_layers = static_cast<int32_t>(spec.layers.size());
+    for (size_t l = 0; l < spec.layers.size() && l < TMC_B200_MAX_LAYERS; ++l) {
+        const auto &y = spec.layers[l];
+        c.layers[l] = tmc_layer{y.n, y.mua, y.mus, y.g, y.d};
+    }
+    tmc_options o{};
+    o.seed = opt.seed;
+    o.batches = static_cast<int32_t>(res.batches.size());
+    const size_t B = res.batches.size(), L = spec.layers.size();
+    std::vector<uint64_t> photons(B);
+    std::vector<double> rd(B), tt(B), absorbed(B * L);
+    for (size_t b = 0; b < B; ++b) {
+        photons[b] = res.batches[b].photons;
+        rd[b] = res.batches[b].rd;
+        tt[b] = res.batches[b].tt;
+        for (size_t l = 0; l < L; ++l) absorbed[b * L + l] = res.batches[b].absorbed[l];
+    }
+    std::vector<double> a_rz = res.a_rz, rd_ra = res.rd_ra, tt_ra = res.tt_ra;
+    tmc_result r{};
+    r.photons = photons.data();
+    r.rd = rd.data();
+    r.tt = tt.data();
+    r.absorbed = absorbed.data();
+    r.a_rz = a_rz.data();
+    r.rd_ra = rd_ra.data();
+    r.tt_ra = tt_ra.data();
+    r.specular = res.specular;
+    r.kernel_seconds = res.kernel_seconds;
+    std::snprintf(r.device, sizeof r.device, "%s", res.device.c_str());
+    tmc_status st{};
+    if (tmc_b200_write_mco(&c, &o, &r, path.c_str(), &st) != TMC_OK) {
+        std::fprintf(stderr, "tissuemc: %s\n", st.message);
+        return false;
+    }
+    return true;
+}
+
 int run_command(int argc, char **argv) {
     if (argc < 3) {
         usage(stderr);
@@ -57,7 +109,7 @@ int run_command(int argc, char **argv) {
     }
     const std::string input = argv[2];
     tissuemc::EngineOptions opt;
-    std::string output;
+    std::string output, mco;
     for (int i = 3; i < argc; ++i) {
         const std::string a = argv[i];
         auto value = [&](const char *name) -> const char * {
@@ -105,6 +157,8 @@ int run_command(int argc, char **argv) {
             }
         } else if (a == "--output") {
             output = value("--output");
+        } else if (a == "--mco") {
+            mco = value("--mco");
         } else {
             std::fprintf(stderr, "tissuemc: unknown option '%s'\n", a.c_str());
             usage(stderr);
@@ -146,6 +200,16 @@ int run_command(int argc, char **argv) {
         if (json.is_open()) {
             if (r) json << ',';
             tissuemc::write_json(res, json);
+        }
+        if (!mco.empty()) {
+            std::string path = mco;
+            if (runs.size() > 1) {
+                const size_t dot = mco.rfind('.');
+                const size_t slash = mco.rfind('/');
+                const bool ext = dot != std::string::npos && (slash == std::string::npos || dot > slash);
+                path = (ext ? mco.substr(0, dot) : mco) + "_" + std::to_string(r + 1) + (ext ? mco.substr(dot) : "");
+            }
+            if (!write_mco(runs[r], opt, res, path)) status = 1;
         }
     }
     if (json.is_open()) {
