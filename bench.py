@@ -1,4 +1,4 @@
-"""Benchmark: photons/s of the MCML photon walk on one B200 (or N replicas, one per GPU).
+"""Benchmark: photons/s of the MCML photon walk on one B200 (or one run sharded over N GPUs).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload skin5|slab_n14] [--impl b200|reference]
 
@@ -11,9 +11,11 @@ memory and are decoded) by the host clock. `cpu_baseline` and `--impl reference`
 reference's own multithreaded CPU engine (oracle/_ref/tissuemc, built from TissueMC's sources) on
 a bounded sample of the same workload on this host's cores.
 
-Under torchrun (N > 1) every rank runs its own replica of the workload (independent seeds): the
-walk has no exchange step, so there is no collective in the data path; ranks meet only at the
-barriers around the timed region, and the slowest rank's time is reported.
+Under torchrun (N > 1) a step is ONE run of N times the workload's photons, sharded by photon id:
+each rank walks its contiguous share (tmc_b200_run_device_range; the same Philox streams and
+batches as on one GPU), then one NCCL all-reduce of the int64 fixed-point tally buffer (1.85 MB
+for skin5) leaves the whole run's tallies on every rank, bit for bit those of a one-GPU run. Work
+per GPU is fixed (weak scaling); the slowest rank's time is reported.
 """
 
 from __future__ import annotations
@@ -269,6 +271,8 @@ def main() -> None:
 
     import torch
 
+    import numpy as np
+
     import tissuemc_b200 as tmc
 
     rank, world, local = _dist()
@@ -283,9 +287,14 @@ def main() -> None:
     spec = tmc.workload(a.workload)
     if a.photons:
         spec.photons = a.photons
-    photons = spec.photons
-    opt = tmc.options(batches=a.batches, seed=1 + 1000003 * rank, device=local,
-                      rung=6 if a.no_profiles else 0, profiles=not a.no_profiles)
+    photons = spec.photons  # per GPU
+    # With N GPUs the job is ONE run of N x photons, sharded by photon id: each rank walks its
+    # contiguous share (the same streams and batches as on one GPU) and one NCCL all-reduce of the
+    # int64 tally buffer gives every rank the whole run's tallies, bit for bit a 1-GPU run's.
+    spec.photons = photons * world
+    first, count = tmc.shard_range(spec.photons, rank, world)
+    opt = tmc.options(batches=a.batches, seed=1, device=local, rung=6 if a.no_profiles else 0,
+                      profiles=not a.no_profiles)
     words = int(tmc.query_sizes(spec, opt).tally_words)
     d_tally = torch.empty(words, dtype=torch.int64, device=f"cuda:{local}")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
@@ -299,12 +308,22 @@ def main() -> None:
             dist.barrier()
             torch.cuda.synchronize()
 
+    def walk() -> None:
+        """This rank's share of the run, then (N > 1) the all-reduce, on `stream`."""
+        if world == 1:
+            tmc.run_device(spec, opt, d_tally.data_ptr(), stream.cuda_stream)
+        else:
+            import torch.distributed as dist
+
+            tmc.run_device_range(spec, opt, first, count, d_tally.data_ptr(), stream.cuda_stream)
+            dist.all_reduce(d_tally)  # unsigned 64-bit sums are int64 two's-complement sums
+
     def step() -> float:
         with torch.cuda.stream(stream):
             flush.fill_(1.0)  # evict L2 between steps (outside the timed events)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            tmc.run_device(spec, opt, d_tally.data_ptr(), stream.cuda_stream)
+            walk()
             e1.record(stream)
         e1.synchronize()
         return e0.elapsed_time(e1)
@@ -323,14 +342,22 @@ def main() -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     ms = total_ms / a.steps
-    value = world * photons / (ms / 1e3)
+    value = spec.photons / (ms / 1e3)
 
-    # end to end through the public C ABI with host buffers
+    # end to end through the public API with host buffers: on one GPU tmc.run (the C ABI's
+    # tmc_b200_run); on N, each rank's shard, the all-reduce, the copy back and the decode
     e2e_times = []
     sz = tmc.query_sizes(spec, opt)
     for i in range(a.steps + 1):
         t0 = time.perf_counter()
-        res = tmc.run(spec, opt)
+        if world == 1:
+            res = tmc.run(spec, opt)
+        else:
+            with torch.cuda.stream(stream):
+                walk()
+            host = d_tally.cpu()  # synchronises the stream
+            res = tmc.decode(spec, opt, host.numpy().view(np.uint64))
+            res.device = torch.cuda.get_device_name(local)
         if i:  # the first call is a warm-up
             e2e_times.append(time.perf_counter() - t0)
     e2e_s = sum(e2e_times) / len(e2e_times)
@@ -340,7 +367,7 @@ def main() -> None:
         t = torch.tensor([e2e_s], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = {"value": world * photons / e2e_s, "unit": "photons/s",
+    e2e = {"value": spec.photons / e2e_s, "unit": "photons/s",
            "h2d_bytes_per_step": int(ctypes.sizeof(tmc.CRunSpec) + ctypes.sizeof(tmc.COptions)),
            "d2h_bytes_per_step": int(sz.tally_words) * 8}
 
@@ -359,10 +386,11 @@ def main() -> None:
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 transport, u64 fixed-point tallies",
             "data": "synthetic (the workload's .mci; seeded Philox photons)",
-            "config": {"workload": f"{a.workload}: {WORKLOADS[a.workload]}", "photons_per_step": photons,
+            "config": {"workload": f"{a.workload}: {WORKLOADS[a.workload]}", "photons_per_step": spec.photons, "photons_per_gpu": photons,
                        "batches": a.batches, "l2": "flushed between steps (256 MB write)",
                        "profiles": not a.no_profiles,
-                       "parallelism": "replicas" if world > 1 else "1 GPU"},
+                       "parallelism": f"one run sharded by photon id over {world} GPUs + NCCL int64 all-reduce"
+                       if world > 1 else "1 GPU"},
             "e2e": e2e,
             "gpu_launches": a.steps,
             "roofline": {

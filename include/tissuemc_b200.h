@@ -153,6 +153,15 @@ TMC_B200_API int tmc_b200_run(const tmc_run_spec *spec, const tmc_options *opt, 
 TMC_B200_API int tmc_b200_run_device(const tmc_run_spec *spec, const tmc_options *opt, uint64_t *d_tally,
                         void *stream, tmc_status *status);
 
+/* One shard of a run: walks only photons [first_photon, first_photon + count) of the run that
+ * spec and opt describe (each with its own stream (seed, id) and its batch in the run's BatchPlan),
+ * into `d_tally` like tmc_b200_run_device. The shards' tally buffers of a partition of [0, photons)
+ * add up (unsigned 64-bit sums) to the whole run's buffer bit for bit, so a run spread over several
+ * GPUs needs one integer all-reduce of the buffer. No reference counterpart (the reference runs on
+ * one GPU, src/cuda/engine.cu:355). */
+TMC_B200_API int tmc_b200_run_device_range(const tmc_run_spec *spec, const tmc_options *opt, uint64_t first_photon,
+                                           uint64_t count, uint64_t *d_tally, void *stream, tmc_status *status);
+
 /* Convert a raw fixed-point tally buffer (as returned in tmc_result.raw or copied back from
  * tmc_b200_run_device) into the result arrays; pure host code. */
 TMC_B200_API int tmc_b200_decode(const tmc_run_spec *spec, const tmc_options *opt, const uint64_t *raw,

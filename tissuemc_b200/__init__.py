@@ -143,6 +143,8 @@ PROTOTYPES = {
     "tmc_b200_parse_mci": (ctypes.c_int, [ctypes.c_char_p, _P(CRunSpec), ctypes.c_int32,
                                           _P(ctypes.c_int32), _P(CStatus)]),
     "tmc_b200_run_static": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _P(CResult), _P(CStatus)]),
+    "tmc_b200_run_device_range": (ctypes.c_int, [_P(CRunSpec), _P(COptions), ctypes.c_uint64, ctypes.c_uint64,
+                                                  ctypes.c_void_p, ctypes.c_void_p, _P(CStatus)]),
     "tmc_b200_write_mco": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _P(CResult), ctypes.c_char_p, _P(CStatus)]),
     "tmc_b200_sweep_default_options": (None, [_P(CSweepOptions)]),
     "tmc_b200_sweep_sample": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int32, _P(CSweepConfig), _P(CStatus)]),
@@ -426,6 +428,23 @@ def run_device(spec: RunSpec, opt: COptions, d_tally_ptr: int, stream_ptr: int =
     c = spec.to_c()
     _check(lib().tmc_b200_run_device(ctypes.byref(c), ctypes.byref(opt), ctypes.c_void_p(d_tally_ptr),
                                      ctypes.c_void_p(stream_ptr), ctypes.byref(st)), st)
+
+
+def run_device_range(spec: RunSpec, opt: COptions, first_photon: int, count: int, d_tally_ptr: int,
+                     stream_ptr: int = 0) -> None:
+    """Launch one shard of a run (photons [first_photon, first_photon + count)) into a device tally
+    buffer on a stream, without synchronising; the shards of a partition add up to the run."""
+    st = CStatus()
+    c = spec.to_c()
+    _check(lib().tmc_b200_run_device_range(ctypes.byref(c), ctypes.byref(opt), first_photon, count,
+                                           ctypes.c_void_p(d_tally_ptr), ctypes.c_void_p(stream_ptr),
+                                           ctypes.byref(st)), st)
+
+
+def shard_range(photons: int, rank: int, world: int) -> tuple[int, int]:
+    """(first photon, count) of rank's contiguous share of a run's photons."""
+    first = photons * rank // world
+    return first, photons * (rank + 1) // world - first
 
 
 def plan(spec: RunSpec, opt: COptions, sms: int = 148, smem_sm: int = 233472,

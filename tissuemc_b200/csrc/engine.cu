@@ -220,6 +220,7 @@ WalkParams make_params(const tmc_run_spec &spec, const tmc_options &opt, const P
     const RunShape sh = shape_of(spec, opt);
     WalkParams P{};
     P.photons = sh.photons;
+    P.id_base = 0u;
     P.seed = opt.seed;
     P.plan_base = static_cast<uint32_t>(sh.photons / static_cast<uint64_t>(sh.nb));
     P.plan_extra = static_cast<uint32_t>(sh.photons % static_cast<uint64_t>(sh.nb));
@@ -261,8 +262,11 @@ WalkParams make_params(const tmc_run_spec &spec, const tmc_options &opt, const P
 namespace {
 
 // Launch the walk on `stream` into `d_tally` (zeroed here). Records ev0/ev1 around it if given.
+// With count > 0, only photons [first, first + count) of the run are walked (a shard: the same
+// streams and batches as in the whole run, so the shards' tallies add up to the run's).
 void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
-                 unsigned long long *d_tally, cudaStream_t stream, cudaEvent_t e0, cudaEvent_t e1) {
+                 unsigned long long *d_tally, cudaStream_t stream, cudaEvent_t e0, cudaEvent_t e1,
+                 uint64_t first = 0, uint64_t count = 0) {
     const RunShape sh = shape_of(spec, opt);
     const size_t words = tally_offsets(sh).total;
     int regs_bps = 0;
@@ -273,11 +277,15 @@ void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
         TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&regs_bps, walk_kernel<0>, threads, 0));
     const Plan pl = make_plan(spec, opt, limits_of(c.prop), regs_bps);
     WalkParams P = make_params(spec, opt, pl, d_tally, reinterpret_cast<unsigned int *>(c.d_counter));
+    if (count) {
+        P.photons = count;
+        P.id_base = static_cast<uint32_t>(first);
+    }
     const size_t smem = plan_smem_bytes(P);
     if (smem > c.prop.sharedMemPerBlockOptin)
         throw Fail(TMC_BAD_CONFIG, "the tally plan does not fit in shared memory");
     // never more lanes than photons: whole blocks only
-    const uint64_t max_blocks = (sh.photons + pl.threads - 1) / pl.threads;
+    const uint64_t max_blocks = (P.photons + pl.threads - 1) / pl.threads;
     const int grid = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(pl.grid), max_blocks));
     if (e0) TMC_CUDA(cudaEventRecord(e0, stream));
     TMC_CUDA(cudaMemsetAsync(d_tally, 0, words * 8, stream));
@@ -402,6 +410,37 @@ int tmc_b200_run(const tmc_run_spec *spec, const tmc_options *opt, tmc_result *r
                       c.prop.minor);
         res->wall_seconds =
             std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return TMC_OK;
+    } catch (const ConfigFailure &e) {
+        set_status(st, TMC_BAD_CONFIG, e.what());
+        return TMC_BAD_CONFIG;
+    } catch (const Fail &e) {
+        set_status(st, e.code(), e.what());
+        return e.code();
+    } catch (const std::exception &e) {
+        set_status(st, TMC_CUDA_ERROR, e.what());
+        return TMC_CUDA_ERROR;
+    }
+}
+
+int tmc_b200_run_device_range(const tmc_run_spec *spec, const tmc_options *opt, uint64_t first_photon,
+                              uint64_t count, uint64_t *d_tally, void *stream, tmc_status *st) {
+    set_status(st, TMC_OK, "");
+    if (!spec || !opt || !d_tally) {
+        set_status(st, TMC_BAD_ARGUMENT, "NULL argument");
+        return TMC_BAD_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    try {
+        validate_run(*spec, *opt);
+        const uint64_t total = shape_of(*spec, *opt).photons;
+        if (count == 0 || first_photon >= total || count > total - first_photon)
+            throw ConfigFailure("photon range [" + std::to_string(first_photon) + ", " +
+                                std::to_string(first_photon + count) + ") is empty or beyond the run's " +
+                                std::to_string(total) + " photons");
+        DeviceCtx &c = device_ctx(opt->device);
+        launch_walk(*spec, *opt, c, reinterpret_cast<unsigned long long *>(d_tally),
+                    static_cast<cudaStream_t>(stream), nullptr, nullptr, first_photon, count);
         return TMC_OK;
     } catch (const ConfigFailure &e) {
         set_status(st, TMC_BAD_CONFIG, e.what());

@@ -42,12 +42,13 @@ static_assert(sizeof(LayerC) == 24 * 4, "LayerC layout");
 
 // Everything the walk kernel needs, passed by value (__grid_constant__).
 struct WalkParams {
-    uint64_t photons;      // photon ids [0, photons), at most 2^31
+    uint64_t photons;      // photons of this launch: ids [id_base, id_base + photons), at most 2^31
     uint64_t seed;         // Philox key
     uint32_t plan_base;    // BatchPlan: photons per batch before the remainder
     uint32_t plan_extra;   // BatchPlan: the first `extra` batches hold one more
     uint32_t plan_bnd;     // BatchPlan: ids below extra * (base + 1) are in the larger batches
     uint32_t threads;      // block size (the random-word ring's stride)
+    uint32_t id_base;      // first photon id (0 for a whole run; a shard of a run starts later)
     unsigned int *counter; // next unclaimed photon id (zeroed before launch)
     unsigned long long *g_batch;   // [nb * (4 + nl)] rd, tt, events, anomalies, absorbed[nl]
     unsigned long long *g_arz;     // [nr * nz]

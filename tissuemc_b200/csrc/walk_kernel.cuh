@@ -185,9 +185,10 @@ __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P
             const bool mine = (need >> lane) & 1u;
             ex_mask |= __ballot_sync(0xffffffffu, mine && my >= n_photons);
             if (mine && my < n_photons) {
-                const int batch = static_cast<int>(my < P.plan_bnd ? my / (P.plan_base + 1u)
-                                                                   : P.plan_extra + (my - P.plan_bnd) / P.plan_base);
-                launch(L, C, my, batch, P.launch_w);
+                const uint32_t id = P.id_base + my;  // the run's photon id: its stream and its batch
+                const int batch = static_cast<int>(id < P.plan_bnd ? id / (P.plan_base + 1u)
+                                                                   : P.plan_extra + (id - P.plan_bnd) / P.plan_base);
+                launch(L, C, id, batch, P.launch_w);
                 alive = true;
             }
         }
