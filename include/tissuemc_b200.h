@@ -330,6 +330,29 @@ TMC_B200_API int tmc_b200_nn_gate(const float *Z, int32_t members, int64_t membe
                                   float threshold, float *rd_mean, float *spread, uint8_t *route, void *stream,
                                   tmc_status *status);
 
+/* Fused ensemble inference (serving): one persistent tcgen05 kernel runs all members of the
+ * surrogate (64 -> 4 x 512 GELU -> 128, BF16 operands, FP32 accumulation in tensor memory) on
+ * tiles of 128 queries, keeping activations on chip, and applies the gate above.
+ *   packed_bytes: size of the packed weight stream for `members` networks (1,769,472 bytes each).
+ *   pack:    weights[m * 5 + l] is member m's layer-l BF16 weight matrix (device, row-major, rows x
+ *            cols = 512 x 64, 512 x 512 three times, 128 x 512; inputs zero-padded to 64 columns,
+ *            outputs to 128 rows); the host array of pointers is read during the call. Re-pack after
+ *            every weight update.
+ *   infer:   bias = members x 2176 floats (the five bias vectors of each member, concatenated);
+ *            feats = n x n_feat raw features, z-scored with x_mean / x_std; outputs de-normalised
+ *            with y_mean / y_std; out (optional) = n x n_out ensemble mean; rd_mean, spread and
+ *            route (optional) as in tmc_b200_nn_gate over the first nbins outputs. Asynchronous on
+ *            `stream`; a bounded tensor-core wait that gives up raises tmc_b200_nn_status. */
+TMC_B200_API int64_t tmc_b200_nn_packed_bytes(int32_t members);
+TMC_B200_API int tmc_b200_nn_pack(const uint16_t *const *weights, int32_t members, uint8_t *packed, void *stream,
+                                  tmc_status *status);
+TMC_B200_API int tmc_b200_nn_ensemble_infer(const uint8_t *packed, const float *bias, int32_t members,
+                                            const float *feats, int32_t n, int32_t n_feat, const float *x_mean,
+                                            const float *x_std, int32_t n_out, const float *y_mean,
+                                            const float *y_std, const float *areas, int32_t nbins, float threshold,
+                                            float *out, float *rd_mean, float *spread, uint8_t *route, void *stream,
+                                            tmc_status *status);
+
 /* Parse an MCML .mci file (the reference's parse_mci_file, src/io/mci.cpp:173-183): writes up to
  * `max_runs` runs and returns the number found in *n_runs. Errors carry the line number. */
 TMC_B200_API int tmc_b200_parse_mci(const char *path, tmc_run_spec *runs, int32_t max_runs, int32_t *n_runs,

@@ -184,3 +184,59 @@ def test_surrogate_beats_monte_carlo_at_equal_cost(trained):
           f"err {err_mc:.4f}")
     assert err_sur < err_mc, (err_sur, err_mc)
     assert t_sur < t_mc, (t_sur, t_mc)
+
+
+def _check_fused_against_layered(S, ens, X):
+    fs = S.FusedServer(ens)
+    spreads: list = []
+    y, rd, route = fs(X, spreads)
+    pm = ens.predict_members(X)  # every member through the per-layer GEMM kernels
+    ref_y = pm.mean(0)
+    # activations are rounded to BF16 in both paths; a last-bit difference in an FP32 sum can round
+    # one activation to its neighbour, so outputs agree to a fraction of a BF16 step
+    assert np.abs(y - ref_y).max() <= 1e-2 * np.abs(ref_y).max()
+    ref_rd = S.rd_total(pm).mean(0)
+    np.testing.assert_allclose(rd, ref_rd, rtol=2e-2)
+    ref_sp = S.spread(pm)
+    sp = spreads[0]
+    assert np.abs(sp - ref_sp).max() <= 2e-3 + 0.05 * ref_sp.max()
+    near = np.abs(ref_sp - fs.threshold) < 2e-3
+    assert np.array_equal(route[~near], (ref_sp > fs.threshold)[~near])
+
+
+def test_fused_ensemble_kernel_matches_the_layered_path_random_weights():
+    """Three untrained members with non-zero biases, 300 queries (a partial last tile)."""
+    from tissuemc_b200 import surrogate as S
+
+    ens = S.Ensemble(members=3, batch=4096, seed=5)
+    rng = np.random.default_rng(7)
+    for m in ens.members:
+        for b in m.b:
+            b.copy_(torch.from_numpy(rng.normal(0, 0.05, b.shape[0]).astype(np.float32)))
+    y_mean = np.concatenate([np.full(S.N_RD, -2.0), [0.05, 0.6]])
+    y_std = np.concatenate([np.full(S.N_RD, 0.3), [0.02, 0.1]])
+    ens.norm = S.Norm(np.zeros(S.N_FEAT), np.ones(S.N_FEAT), y_mean, y_std)
+    X = rng.normal(size=(300, S.N_FEAT))
+    _check_fused_against_layered(S, ens, X)
+
+
+def test_fused_ensemble_kernel_matches_the_layered_path_trained(trained):
+    """The trained ensemble on 40,000 queries: more tiles of 128 than SMs, so every CTA of the
+    persistent kernel walks several tiles."""
+    S, ens, _, (Xv, _) = trained
+    X = np.tile(Xv, (20, 1))[:40_000]
+    _check_fused_against_layered(S, ens, X)
+
+
+def test_fused_ensemble_rejects_bad_shapes():
+    from tissuemc_b200 import surrogate as S
+    import ctypes
+
+    dummy = torch.zeros(16, device="cuda")
+    p = S._p(dummy)
+    with pytest.raises(tmc.ConfigError, match="1-8 members"):
+        S._call("tmc_b200_nn_ensemble_infer", p, p, 9, p, 10, 13, p, p, 66, p, p, p, 64, ctypes.c_float(0.01),
+                p, p, p, p, ctypes.c_void_p(0))
+    with pytest.raises(tmc.ConfigError, match="R_d bins"):
+        S._call("tmc_b200_nn_ensemble_infer", p, p, 4, p, 10, 13, p, p, 66, p, p, p, 65, ctypes.c_float(0.01),
+                p, p, p, p, ctypes.c_void_p(0))

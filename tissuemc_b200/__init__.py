@@ -174,6 +174,14 @@ PROTOTYPES = {
     "tmc_b200_nn_gate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32] +
                          [ctypes.c_void_p] * 3 + [ctypes.c_int32, ctypes.c_int32, ctypes.c_float] +
                          [ctypes.c_void_p] * 4 + [_P(CStatus)]),
+    "tmc_b200_nn_packed_bytes": (ctypes.c_int64, [ctypes.c_int32]),
+    "tmc_b200_nn_pack": (ctypes.c_int, [_P(ctypes.c_void_p), ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                        _P(CStatus)]),
+    "tmc_b200_nn_ensemble_infer": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                                  ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_int32, ctypes.c_float] + [ctypes.c_void_p] * 5 +
+                                   [_P(CStatus)]),
     "tmc_b200_plan": (ctypes.c_int, [_P(CRunSpec), _P(COptions), ctypes.c_int32, ctypes.c_int64,
                                      ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _P(CPlan),
                                      _P(CStatus)]),

@@ -17,6 +17,7 @@
 
 #include "../../include/tissuemc_b200.h"
 #include "gemm_tc.cuh"
+#include "mlp_infer.cuh"
 
 namespace tmc {
 namespace {
@@ -176,6 +177,7 @@ __global__ void gate_kernel(const float *__restrict__ Z, int members, size_t mem
 std::mutex g_mu;
 int *g_status[64] = {};
 bool g_attr[64] = {};
+bool g_infer_attr[64] = {};
 
 void put(tmc_status *st, int code, const std::string &m) {
     if (!st) return;
@@ -399,6 +401,98 @@ int tmc_b200_nn_gate(const float *Z, int32_t members, int64_t member_stride, int
     gate_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
         Z, members, static_cast<size_t>(member_stride), ld, ymean, ystd, areas, nbins, n, threshold, rd_mean, spread,
         route);
+    return launched(st);
+}
+
+int64_t tmc_b200_nn_packed_bytes(int32_t members) {
+    return members < 1 ? 0 : static_cast<int64_t>(members) * kInferMemberBytes;
+}
+
+int tmc_b200_nn_pack(const uint16_t *const *weights, int32_t members, uint8_t *packed, void *stream,
+                     tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!weights || !packed) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument");
+        return TMC_BAD_ARGUMENT;
+    }
+    if (members < 1 || members > kInferMaxMembers) {
+        put(st, TMC_BAD_CONFIG, "the fused ensemble holds 1 to 8 members");
+        return TMC_BAD_CONFIG;
+    }
+    PackParams P{};
+    P.members = members;
+    for (int i = 0; i < members * kInferLayers; ++i) {
+        if (!weights[i] || reinterpret_cast<uintptr_t>(weights[i]) % 16 != 0) {
+            put(st, TMC_BAD_ARGUMENT, "every weight matrix must be a non-NULL, 16-byte aligned device pointer");
+            return TMC_BAD_ARGUMENT;
+        }
+        P.w[i] = reinterpret_cast<const __nv_bfloat16 *>(weights[i]);
+    }
+    const size_t units = static_cast<size_t>(members) * (kInferMemberBytes / 16);
+    pack_kernel<<<static_cast<unsigned>((units + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(P, packed);
+    return launched(st);
+}
+
+int tmc_b200_nn_ensemble_infer(const uint8_t *packed, const float *bias, int32_t members, const float *feats, int32_t n,
+                               int32_t n_feat, const float *x_mean, const float *x_std, int32_t n_out,
+                               const float *y_mean, const float *y_std, const float *areas, int32_t nbins,
+                               float threshold, float *out, float *rd_mean, float *spread, uint8_t *route,
+                               void *stream, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!packed || !bias || !x_mean || !x_std || !y_mean || !y_std || (n > 0 && !feats) || (nbins > 0 && !areas)) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument");
+        return TMC_BAD_ARGUMENT;
+    }
+    if (members < 1 || members > kInferMaxMembers || n < 0 || n_feat < 1 || n_feat > kInferIn || n_out < 1 ||
+        n_out > kInferOut || nbins < 0 || nbins > 64 || nbins > n_out) {
+        put(st, TMC_BAD_CONFIG,
+            "fused ensemble: 1-8 members, 1-64 input features, 1-128 outputs, 0-64 R_d bins among the outputs");
+        return TMC_BAD_CONFIG;
+    }
+    if (n == 0) return TMC_OK;
+    if (reinterpret_cast<uintptr_t>(packed) % 16 != 0) {
+        put(st, TMC_BAD_ARGUMENT, "the packed weights must be 16-byte aligned");
+        return TMC_BAD_ARGUMENT;
+    }
+    const int dev = current_device();
+    int sms = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        if (!status_word(dev) || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            put(st, TMC_NO_DEVICE, "no usable CUDA device found");
+            return TMC_NO_DEVICE;
+        }
+        if (!g_infer_attr[dev]) {
+            if (cudaFuncSetAttribute(ensemble_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     InferSmem::bytes) != cudaSuccess)
+                return launched(st);
+            g_infer_attr[dev] = true;
+        }
+    }
+    InferParams P{};
+    P.packed = packed;
+    P.bias = bias;
+    P.feats = feats;
+    P.x_mean = x_mean;
+    P.x_std = x_std;
+    P.y_mean = y_mean;
+    P.y_std = y_std;
+    P.areas = areas;
+    P.out = out;
+    P.rd_mean = rd_mean;
+    P.spread = spread;
+    P.route = route;
+    P.n = n;
+    P.n_feat = n_feat;
+    P.n_out = n_out;
+    P.nbins = nbins;
+    P.members = members;
+    P.threshold = threshold;
+    P.status = g_status[dev];
+    const int tiles = (n + 127) / 128;
+    const int grid = tiles < sms ? tiles : sms;  // persistent: one CTA per SM (its shared memory allows no more)
+    ensemble_infer_kernel<<<grid, kInferThreads, InferSmem::bytes, static_cast<cudaStream_t>(stream)>>>(P);
     return launched(st);
 }
 

@@ -336,6 +336,80 @@ class Server:
         return y, t.cat(rds).numpy(), t.cat(routes).numpy().astype(bool)
 
 
+class FusedServer:
+    """Gated serving through the fused ensemble kernel (tmc_b200_nn_ensemble_infer): every
+    member's five layers and the gate run in one persistent tcgen05 launch per call, activations
+    stay on chip, and only raw features go in and the ensemble's outputs, mean R_d, spread and route
+    flags come out. The members' weights are packed once (re-create the server after training)."""
+
+    def __init__(self, ens: Ensemble, threshold: float = 0.01):
+        import torch
+
+        t = self.torch = torch
+        self.ens, self.threshold = ens, threshold
+        dev = ens.dev
+        M = len(ens.members)
+        self.members = M
+        self.packed = t.empty(int(lib().tmc_b200_nn_packed_bytes(M)), dtype=t.uint8, device=dev)
+        ptrs = (ctypes.c_void_p * (M * len(LAYER_DIMS)))(*[m.Wb[li].data_ptr() for m in ens.members
+                                                           for li in range(len(LAYER_DIMS))])
+        s = t.cuda.current_stream().cuda_stream
+        _call("tmc_b200_nn_pack", ptrs, M, _p(self.packed), ctypes.c_void_p(s))
+        self.bias = t.cat([t.cat(m.b) for m in ens.members]).contiguous()
+        nm = ens.norm
+        f32 = dict(dtype=t.float32, device=dev)
+        self.x_mean, self.x_std = t.tensor(nm.x_mean, **f32), t.tensor(nm.x_std, **f32)
+        self.y_mean, self.y_std = t.tensor(nm.y_mean, **f32), t.tensor(nm.y_std, **f32)
+        self.areas = t.tensor(annulus_areas(), **f32)
+        self.cap = 0
+
+    def _reserve(self, n: int) -> None:
+        if n <= self.cap:
+            return
+        t, dev = self.torch, self.ens.dev
+        self.cap = n
+        self.d_feats = t.empty(n, N_FEAT, dtype=t.float32, device=dev)
+        self.d_out = t.empty(n, N_OUT, dtype=t.float32, device=dev)
+        self.d_rd = t.empty(n, dtype=t.float32, device=dev)
+        self.d_spread = t.empty(n, dtype=t.float32, device=dev)
+        self.d_route = t.empty(n, dtype=t.uint8, device=dev)
+        self.h_feats = t.empty(n, N_FEAT, dtype=t.float32, pin_memory=True)
+        self.h_out = t.empty(n, N_OUT, dtype=t.float32, pin_memory=True)
+        self.h_rd = t.empty(n, dtype=t.float32, pin_memory=True)
+        self.h_spread = t.empty(n, dtype=t.float32, pin_memory=True)
+        self.h_route = t.empty(n, dtype=t.uint8, pin_memory=True)
+
+    def launch(self, d_feats, n: int, d_out, d_rd, d_spread, d_route, stream: int) -> None:
+        """The kernel alone, on device buffers."""
+        _call("tmc_b200_nn_ensemble_infer", _p(self.packed), _p(self.bias), self.members, _p(d_feats), n, N_FEAT,
+              _p(self.x_mean), _p(self.x_std), N_OUT, _p(self.y_mean), _p(self.y_std), _p(self.areas), N_RD,
+              ctypes.c_float(self.threshold), _p(d_out), _p(d_rd), _p(d_spread), _p(d_route), ctypes.c_void_p(stream))
+
+    def __call__(self, feats: np.ndarray, spreads: list | None = None):
+        """(mean raw outputs (n, 66), mean R_d on the grid (n,), route flags (n,)); the spreads are
+        appended to `spreads` when it is given. Host to device, kernel and device to host on the
+        current stream, synchronised at the end."""
+        t = self.torch
+        n = len(feats)
+        self._reserve(n)
+        s = t.cuda.current_stream()
+        self.h_feats[:n].numpy()[:] = feats
+        self.d_feats[:n].copy_(self.h_feats[:n], non_blocking=True)
+        self.launch(self.d_feats, n, self.d_out, self.d_rd, self.d_spread, self.d_route, s.cuda_stream)
+        self.h_out[:n].copy_(self.d_out[:n], non_blocking=True)
+        self.h_rd[:n].copy_(self.d_rd[:n], non_blocking=True)
+        self.h_route[:n].copy_(self.d_route[:n], non_blocking=True)
+        if spreads is not None:
+            self.h_spread[:n].copy_(self.d_spread[:n], non_blocking=True)
+        s.synchronize()
+        if lib().tmc_b200_nn_status(1):
+            raise RuntimeError("a tensor-core wait gave up in the fused ensemble kernel")
+        if spreads is not None:
+            spreads.append(self.h_spread[:n].numpy().copy())
+        return (self.h_out[:n].numpy().astype(np.float64), self.h_rd[:n].numpy().copy(),
+                self.h_route[:n].numpy().astype(bool))
+
+
 def spread(members_out: np.ndarray) -> np.ndarray:
     """The members' disagreement on the predicted diffuse reflectance: sample standard deviation
     over the mean of each member's R_d on the grid."""
