@@ -41,7 +41,9 @@ WORKLOADS = {
     "slab_n14": "single slab n=1.4 in air (mua=5, mus=95, g=0.8, d=0.05 cm; 1e6 photons; 50x20 grid, na=30)",
     "sweep": SWEEP_DESC,
     "surrogate": "learned surrogate trained on sweep solves; gated serving and inverse fits",
+    "serve": "fused ensemble inference: 4 members of 13(64) -> 4x512 GELU -> 66(128), gate on the R_d spread",
 }
+SERVE_FLOP_PER_QUERY = 4 * 2 * (64 * 512 + 3 * 512 * 512 + 512 * 128)  # 7.08 MFLOP (padded shapes)
 METRIC = "photons/s on 1 B200 (plain MC)"
 
 # Algorithmic work of the walk, counted from the reference's step (include/tissuemc/physics.hpp
@@ -68,6 +70,7 @@ def _args():
     ap.add_argument("--autotune", action="store_true", help="sweep: pick the launch shape first")
     ap.add_argument("--scale", type=float, default=1.0, help="surrogate: fraction of the full data and query counts")
     ap.add_argument("--epochs", type=int, default=20, help="surrogate: training epochs")
+    ap.add_argument("--queries", type=int, default=1 << 20, help="serve: queries per step")
     ap.add_argument("--no-profiles", action="store_true",
                     help="diagnostic: skip the profile tallies (rung 6 without profiles); not a result")
     return ap.parse_args()
@@ -256,6 +259,76 @@ def run_surrogate(a) -> None:
             "speedup_vs_plain_mc": s["speedup_vs_plain_mc"], "details": res}), flush=True)
 
 
+def run_serve(a) -> None:
+    """Surrogate serving throughput: one fused tcgen05 launch (tmc_b200_nn_ensemble_infer) per
+    step over --queries feature vectors drawn from the sweep distribution. The weights are random
+    (the kernel's work does not depend on their values). value = queries / CUDA-event time of the
+    launch, L2 flushed between steps; e2e = queries / host time of FusedServer (pinned host
+    features in, host outputs, mean R_d and route flags out)."""
+    import numpy as np
+    import torch
+
+    import tissuemc_b200 as tmc
+    from tissuemc_b200 import surrogate as S
+
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    n = a.queries
+    ens = S.Ensemble(members=4, batch=4096, seed=0, device=f"cuda:{local}")
+    ens.norm = S.Norm(np.zeros(S.N_FEAT), np.ones(S.N_FEAT), np.full(S.N_OUT, -2.0), np.full(S.N_OUT, 0.3))
+    q = S.features(tmc.sweep_sample(3000 + rank, n))
+    q = (q - q.mean(0)) / np.maximum(q.std(0), 1e-6)
+    fs = S.FusedServer(ens)
+    fs._reserve(n)
+    fs.d_feats[:n].copy_(torch.from_numpy(q.astype(np.float32)))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream()
+
+    def step() -> float:
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fs.launch(fs.d_feats, n, fs.d_out, fs.d_rd, fs.d_spread, fs.d_route, stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(a.warmup):
+        step()
+    with Clocks(local) as clk:
+        times = [step() for _ in range(a.steps)]
+    if tmc.lib().tmc_b200_nn_status(1):
+        raise RuntimeError("a tensor-core wait gave up in the fused ensemble kernel")
+    ms = sum(times) / len(times)
+    e2e_t = []
+    for i in range(a.steps + 1):
+        t0 = time.perf_counter()
+        fs(q)
+        if i:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_s = sum(e2e_t) / len(e2e_t)
+    if rank == 0:
+        peaks = _peaks()
+        peak = float(peaks.get("bf16_tflops", 1590.0))
+        achieved = n * SERVE_FLOP_PER_QUERY / (ms * 1e-3) / 1e12
+        print(json.dumps({
+            "metric": "surrogate queries/s on 1 B200 (fused ensemble kernel)", "value": n / (ms * 1e-3),
+            "unit": "queries/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 operands, fp32 accumulation", "data": "synthetic (sweep-distribution queries, random weights)",
+            "config": {"workload": f"serve: {WORKLOADS['serve']}", "queries_per_step": n,
+                       "l2": "flushed between steps (256 MB write)"},
+            "e2e": {"value": n / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": n * S.N_FEAT * 4,
+                    "d2h_bytes_per_step": n * (S.N_OUT * 4 + 4 + 1)},
+            "gpu_launches": a.steps,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": "bf16_tflops (burst) of MEASURED_PEAKS.json; algorithmic FLOPs of the "
+                                        "padded layers, 7.08 MFLOP per query"},
+            "clocks": clk.summary(),
+        }), flush=True)
+
+
 def main() -> None:
     a = _args()
     if a.impl == "reference":
@@ -266,6 +339,9 @@ def main() -> None:
         return
     if a.workload == "sweep":
         run_sweep(a)
+        return
+    if a.workload == "serve":
+        run_serve(a)
         return
     import ctypes
 

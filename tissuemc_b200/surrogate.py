@@ -540,7 +540,7 @@ def pipeline(scale: float = 1.0, members: int = 4, epochs: int = 20, seed: int =
     n_q = max(65536, int(1_000_000 * scale))
     qcfg = sweep_sample(3000 + seed, n_q)
     Xq = features(qcfg)
-    server = Server(ens)
+    server = FusedServer(ens)
     server(Xq[:65536])  # warm-up
     torch.cuda.synchronize()
     t0 = time.perf_counter()
