@@ -299,6 +299,8 @@ TMC_B200_API int tmc_b200_gemm_bf16(const uint16_t *A, const uint16_t *B, const 
  *                optional) = 2 scale (pred - target), zero in the padded columns.
  * adam:          one Adam step (lr_t already bias-corrected) on float32 master weights, writing
  *                the bf16 copy wb and its transpose wt (each optional).
+ * ema:           avg = beta avg + (1 - beta) w over n float32 values (Polyak averaging).
+ * to_bf16:       wb = bf16(w) and wt = its transpose (each optional) for a rows x cols matrix.
  * status:        nonzero if a bounded tensor-core wait gave up since the last clear. */
 TMC_B200_API int tmc_b200_nn_linear(const uint16_t *X, const uint16_t *W, const float *bias, float *Z, uint16_t *H,
                                     int32_t M, int32_t N, int32_t K, int32_t gelu, void *stream, tmc_status *status);
@@ -315,6 +317,9 @@ TMC_B200_API int tmc_b200_nn_mse(const float *pred, const float *target, uint16_
 TMC_B200_API int tmc_b200_nn_adam(float *w, const float *g, float *m, float *v, int32_t rows, int32_t cols,
                                   float lr_t, float b1, float b2, float eps, float weight_decay, uint16_t *wb,
                                   uint16_t *wt, void *stream, tmc_status *status);
+TMC_B200_API int tmc_b200_nn_ema(const float *w, float *avg, int64_t n, float beta, void *stream, tmc_status *status);
+TMC_B200_API int tmc_b200_nn_to_bf16(const float *w, int32_t rows, int32_t cols, uint16_t *wb, uint16_t *wt,
+                                     void *stream, tmc_status *status);
 TMC_B200_API int tmc_b200_nn_status(int32_t clear);
 /* encode: X (n x ld, bf16) = z-scored feats (n x nf, float32), zero-padded to ld columns.
  * gate:   per query, each member's diffuse reflectance on the grid from its normalised outputs

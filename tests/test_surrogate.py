@@ -143,7 +143,7 @@ def test_gate_flags_disagreement_out_of_distribution(trained):
 
 def test_inverse_fit_recovers_parameters_through_the_surrogate(trained):
     S, ens, _, (Xv, _) = trained
-    two = Xv[(Xv[:, 7] > 0) & (Xv[:, 11] == 0)][:64].copy()  # two-layer configurations
+    two = Xv[S.present(Xv, 1) & ~S.present(Xv, 2)][:64].copy()  # two-layer configurations
     assert len(two) >= 16
     obs = ens.predict(two)[:, :S.N_RD]  # noise-free, self-consistent observations
     mask = (obs > -3.5).astype(float)

@@ -138,6 +138,20 @@ __global__ void adam_kernel(float *__restrict__ w, const float *__restrict__ g, 
     }
 }
 
+__global__ void ema_kernel(const float *__restrict__ w, float *__restrict__ avg, size_t n, float beta) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) avg[i] = beta * avg[i] + (1.0f - beta) * w[i];
+}
+
+__global__ void to_bf16_kernel(const float *__restrict__ w, int rows, int cols, __nv_bfloat16 *wb,
+                               __nv_bfloat16 *wt) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= static_cast<size_t>(rows) * cols) return;
+    const __nv_bfloat16 b = __float2bfloat16_rn(w[i]);
+    if (wb) wb[i] = b;
+    if (wt) wt[static_cast<size_t>(i % cols) * rows + i / cols] = b;
+}
+
 // Network inputs from raw features: z-score the first nf of n_feat columns, zero-pad to ld, bf16.
 __global__ void encode_kernel(const float *__restrict__ feats, const float *__restrict__ mean,
                               const float *__restrict__ stdv, __nv_bfloat16 *__restrict__ X, int n, int nf, int ld) {
@@ -374,6 +388,30 @@ int tmc_b200_nn_adam(float *w, const float *g, float *m, float *v, int32_t rows,
     adam_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         w, g, m, v, rows, cols, lr_t, b1, b2, eps, weight_decay, reinterpret_cast<__nv_bfloat16 *>(wb),
         reinterpret_cast<__nv_bfloat16 *>(wt));
+    return launched(st);
+}
+
+int tmc_b200_nn_ema(const float *w, float *avg, int64_t n, float beta, void *stream, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!w || !avg || n < 1) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument or empty parameter");
+        return TMC_BAD_ARGUMENT;
+    }
+    ema_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        w, avg, static_cast<size_t>(n), beta);
+    return launched(st);
+}
+
+int tmc_b200_nn_to_bf16(const float *w, int32_t rows, int32_t cols, uint16_t *wb, uint16_t *wt, void *stream,
+                        tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!w || rows < 1 || cols < 1) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument or empty parameter");
+        return TMC_BAD_ARGUMENT;
+    }
+    const size_t n = static_cast<size_t>(rows) * cols;
+    to_bf16_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        w, rows, cols, reinterpret_cast<__nv_bfloat16 *>(wb), reinterpret_cast<__nv_bfloat16 *>(wt));
     return launched(st);
 }
 

@@ -8,8 +8,9 @@ the network — forward, backward, loss, Adam — runs in this package's CUDA ke
 bias/GELU epilogues); torch only provides device buffers, random permutations and gathers.
 
 Encoding (13 inputs, 66 outputs):
-  inputs   for layer slots 0..2: log10 mu_a, log10 mu_s', g, thickness d (zeros for an absent
-           layer: d = 0 marks it), then the shared refractive index n; z-scored, zero-padded to 64.
+  inputs   for layer slots 0..2: log10 mu_a, log10 mu_s', g, log10 thickness (an absent layer:
+           zeros, and log10 thickness ABSENT_LOG_D), then the shared refractive index n;
+           z-scored, zero-padded to 64.
   outputs  log10 of R_d(r) per unit area [1/cm^2] in the 64 radial bins (floored at 1e-4), then
            T_t and A per photon; z-scored.
 """
@@ -28,6 +29,10 @@ N_FEAT, K_IN, HIDDEN, N_HIDDEN = 13, 64, 512, 4
 N_RD = 64
 N_OUT, N_OUT_PAD = N_RD + 2, 128
 RD_FLOOR = 1e-4
+# Thickness enters as log10(d) (d is drawn log-uniformly in [0.01, 1] cm); an absent layer slot has
+# log10(d) = ABSENT_LOG_D, a decade below the thinnest layer, and zeros elsewhere.
+LOG_THICKNESS = True
+ABSENT_LOG_D = -3.0
 LAYER_DIMS = [(K_IN, HIDDEN)] + [(HIDDEN, HIDDEN)] * (N_HIDDEN - 1) + [(HIDDEN, N_OUT_PAD)]  # (in, out)
 
 
@@ -52,10 +57,27 @@ def features(cfgs) -> np.ndarray:
     with np.errstate(divide="ignore", invalid="ignore"):
         block = np.stack([np.log10(lay[..., 1]), np.log10(lay[..., 2] * (1.0 - lay[..., 3])), lay[..., 3],
                           lay[..., 4]], axis=-1)
+    if LOG_THICKNESS:
+        with np.errstate(divide="ignore", invalid="ignore"):
+            block[..., 3] = np.log10(lay[..., 4])
     block[~present] = 0.0
+    if LOG_THICKNESS:
+        block[..., 3][~present] = ABSENT_LOG_D
     out[:, :12] = block.reshape(len(a), 12)
     out[:, 12] = lay[:, 0, 0]
     return out
+
+
+def present(X: np.ndarray, layer: int) -> np.ndarray:
+    """Which rows of raw features have layer slot `layer` (0..2)."""
+    d = X[:, 4 * layer + 3]
+    return d > ABSENT_LOG_D + 0.5 if LOG_THICKNESS else d > 0
+
+
+def thickness(X: np.ndarray, layer: int) -> np.ndarray:
+    """Thickness [cm] of layer slot `layer` (0 where absent)."""
+    d = X[:, 4 * layer + 3]
+    return np.where(present(X, layer), 10.0 ** d if LOG_THICKNESS else d, 0.0)
 
 
 def annulus_areas(nr: int = N_RD, dr: float = 0.01) -> np.ndarray:
@@ -212,8 +234,11 @@ class Ensemble:
         return t.from_numpy(Xn).to(self.dev).to(t.bfloat16)
 
     def train(self, X: np.ndarray, Y: np.ndarray, epochs: int, lr: float = 1e-3, seed: int = 0,
-              lr_final: float = 1e-5) -> list[float]:
-        """Adam with a cosine learning-rate decay; returns the mean training loss per epoch."""
+              lr_final: float = 1e-5, ema: float = 0.0) -> list[float]:
+        """Adam with a cosine learning-rate decay; returns the mean training loss per epoch. With
+        ema > 0 every member also keeps an exponential moving average of its weights (Polyak
+        averaging, avg = ema avg + (1 - ema) w after each step), which replaces the weights at the
+        end."""
         t = self.torch
         self.norm = Norm.fit(X, Y)
         Xd = self._x(X)
@@ -229,12 +254,15 @@ class Ensemble:
         xb = t.empty(self.B, K_IN, dtype=t.bfloat16, device=self.dev)
         yb = t.empty(self.B, N_OUT, dtype=t.float32, device=self.dev)
         k = 0
+        avg = []
+        if ema > 0:
+            avg = [([w.clone() for w in m.W], [b.clone() for b in m.b]) for m in self.members]
         for _ in range(epochs):
             perms = [t.randperm(n, generator=gen, device=self.dev) for _ in self.members]
             acc = t.zeros(1, dtype=t.float32, device=self.dev)
             for s in range(steps):
                 lr_k = lr_final + 0.5 * (lr - lr_final) * (1 + math.cos(math.pi * k / total))
-                for m, perm in zip(self.members, perms, strict=True):
+                for mi, (m, perm) in enumerate(zip(self.members, perms, strict=True)):
                     idx = perm[s * self.B:(s + 1) * self.B]
                     t.index_select(Xd, 0, idx, out=xb)
                     t.index_select(Yd, 0, idx, out=yb)
@@ -242,8 +270,20 @@ class Ensemble:
                     m.backward(xb, yb, stream, scale)
                     m.adam(stream, lr_k)
                     acc += m.loss
+                    if avg:
+                        aw, ab = avg[mi]
+                        for p, q in zip(m.W + m.b, aw + ab, strict=True):
+                            _call("tmc_b200_nn_ema", _p(p), _p(q), p.numel(), ctypes.c_float(ema),
+                                  ctypes.c_void_p(stream))
                 k += 1
             self.history.append(float(acc.item()) / (steps * len(self.members)))
+        for m, (aw, ab) in zip(self.members, avg):
+            for li, (w, b) in enumerate(zip(aw, ab, strict=True)):
+                m.W[li].copy_(w)
+                m.b[li].copy_(b)
+                n_out, k_in = LAYER_DIMS[li][1], LAYER_DIMS[li][0]
+                _call("tmc_b200_nn_to_bf16", _p(m.W[li]), n_out, k_in, _p(m.Wb[li]), _p(m.WT[li]),
+                      ctypes.c_void_p(stream))
         if lib().tmc_b200_nn_status(1):
             raise RuntimeError("a tensor-core wait gave up during training")
         return self.history
@@ -470,9 +510,9 @@ def config_from_features(f: np.ndarray, photons: int, seed: int) -> CSweepConfig
     c.photons, c.seed, c.n_above, c.n_below = photons, seed, 1.0, 1.0
     nl = 0
     for l in range(3):
-        d = f[4 * l + 3]
-        if d <= 0:
+        if not present(f[None, :], l)[0]:
             break
+        d = float(thickness(f[None, :], l)[0])
         g = f[4 * l + 2]
         c.layers[l] = Layer(f[12], 10 ** f[4 * l], 10 ** f[4 * l + 1] / (1 - g), g, d)
         nl += 1
