@@ -71,6 +71,10 @@ def _args():
     ap.add_argument("--scale", type=float, default=1.0, help="surrogate: fraction of the full data and query counts")
     ap.add_argument("--epochs", type=int, default=20, help="surrogate: training epochs")
     ap.add_argument("--queries", type=int, default=1 << 20, help="serve: queries per step")
+    ap.add_argument("--configs", type=int, default=4096, help="sweep: configurations")
+    ap.add_argument("--photon-scale", type=float, default=1.0, help="sweep: scale every configuration's photons "
+                    "(diagnostic)")
+    ap.add_argument("--no-loop", action="store_true", help="sweep: skip the single-run loop baseline (diagnostic)")
     ap.add_argument("--no-profiles", action="store_true",
                     help="diagnostic: skip the profile tallies (rung 6 without profiles); not a result")
     return ap.parse_args()
@@ -207,7 +211,10 @@ def run_sweep(a) -> None:
     import tissuemc_b200 as tmc
 
     rank, world, local = _dist()
-    cfgs = tmc.sweep_sample(1 + rank, 4096)
+    cfgs = tmc.sweep_sample(1 + rank, a.configs)
+    if a.photon_scale != 1.0:  # diagnostic: a shorter sweep over the same configurations
+        for c in cfgs:
+            c.photons = max(1, int(c.photons * a.photon_scale))
     opt = tmc.sweep_options(device=local)
     if a.autotune:
         opt, _ = tmc.sweep_autotune(cfgs, opt)
@@ -220,7 +227,7 @@ def run_sweep(a) -> None:
             r = tmc.sweep_run(cfgs, opt)
             wall.append(time.perf_counter() - t0)
             kern.append(r.seconds)
-    loop = tmc.sweep_run_loop(cfgs, opt).seconds
+    loop = None if a.no_loop else tmc.sweep_run_loop(cfgs, opt).seconds
     n = len(cfgs)
     ks, ws = sum(kern) / len(kern), sum(wall) / len(wall)
     if rank == 0:
@@ -229,14 +236,16 @@ def run_sweep(a) -> None:
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * ks,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 transport, u64 fixed-point tallies", "data": "synthetic (seeded configurations)",
-            "config": {"workload": f"sweep: {SWEEP_DESC}", "threads_per_block": opt.threads_per_block,
+            "config": {"workload": f"sweep: {SWEEP_DESC}", "configs": n, "photon_scale": a.photon_scale,
+                       "threads_per_block": opt.threads_per_block,
                        "item_photons": opt.item_photons, "autotuned": bool(a.autotune)},
             "e2e": {"value": world * n / ws, "unit": "solves/s",
                     "h2d_bytes_per_step": n * 48 + n * 4 + sum(c.num_layers for c in cfgs) * 96,
                     "d2h_bytes_per_step": n * (opt.nr + 3) * 8},
-            "loop_baseline": {"value": n / loop, "unit": "solves/s", "seconds": loop,
-                              "what": "one single-run walk launch per configuration, back to back on one stream"},
-            "speedup_vs_loop": loop / ks,
+            "loop_baseline": None if loop is None else {
+                "value": n / loop, "unit": "solves/s", "seconds": loop,
+                "what": "one single-run walk launch per configuration, back to back on one stream"},
+            "speedup_vs_loop": None if loop is None else loop / ks,
             "photons_per_s": sum(int(c.photons) for c in cfgs) / ks,
             "gpu_launches": a.steps * 2, "clocks": clk.summary(),
         }), flush=True)
