@@ -296,17 +296,23 @@ __global__ void __launch_bounds__(kInferThreads, 1) ensemble_infer_kernel(const 
                     }
                     tc_fence_after();
                     if (l < 4) {
-                        // hidden layer: columns [128 j, 128 j + 128) of 512
-                        const float *b = bias + l * kInferHidden;
+                        // hidden layer: columns [128 j, 128 j + 128) of 512, 16 at a time; the bias
+                        // as 16-byte vector loads (one address across the warp)
+                        const float4 *b4 = reinterpret_cast<const float4 *>(bias + l * kInferHidden);
 #pragma unroll 1
                         for (int c0 = j * 128; c0 < j * 128 + 128; c0 += 16) {
+                            float4 bb[4];
+#pragma unroll
+                            for (int i = 0; i < 4; ++i) bb[i] = __ldg(b4 + (c0 >> 2) + i);
                             float v[16];
                             tmem_ld16(lane_addr + static_cast<uint32_t>(c0), v);
                             uint32_t w[8];
 #pragma unroll
-                            for (int i = 0; i < 8; ++i)
-                                w[i] = pack_bf16x2(infer_gelu(v[2 * i] + __ldg(b + c0 + 2 * i)),
-                                                   infer_gelu(v[2 * i + 1] + __ldg(b + c0 + 2 * i + 1)));
+                            for (int i = 0; i < 4; ++i) {
+                                w[2 * i] = pack_bf16x2(infer_gelu(v[4 * i] + bb[i].x), infer_gelu(v[4 * i + 1] + bb[i].y));
+                                w[2 * i + 1] =
+                                    pack_bf16x2(infer_gelu(v[4 * i + 2] + bb[i].z), infer_gelu(v[4 * i + 3] + bb[i].w));
+                            }
                             *reinterpret_cast<uint4 *>(act_unit(A, r, c0)) = make_uint4(w[0], w[1], w[2], w[3]);
                             *reinterpret_cast<uint4 *>(act_unit(A, r, c0 + 8)) = make_uint4(w[4], w[5], w[6], w[7]);
                         }

@@ -425,29 +425,46 @@ class FusedServer:
               _p(self.x_mean), _p(self.x_std), N_OUT, _p(self.y_mean), _p(self.y_std), _p(self.areas), N_RD,
               ctypes.c_float(self.threshold), _p(d_out), _p(d_rd), _p(d_spread), _p(d_route), ctypes.c_void_p(stream))
 
-    def __call__(self, feats: np.ndarray, spreads: list | None = None):
-        """(mean raw outputs (n, 66), mean R_d on the grid (n,), route flags (n,)); the spreads are
-        appended to `spreads` when it is given. Host to device, kernel and device to host on the
-        current stream, synchronised at the end."""
+    def __call__(self, feats, spreads: list | None = None, copy: bool = True, chunk: int = 131072):
+        """(mean raw outputs (n, 66), mean R_d on the grid (n,), route flags (n,)) as float32 /
+        bool arrays; the spreads are appended to `spreads` when it is given. `feats` is an (n, 13)
+        array, or a pinned float32 torch tensor used in place. The queries go through in chunks on
+        two streams, so that one chunk's copies overlap another's kernel; the call returns when all
+        results are on the host. With copy=False the arrays are views of this server's pinned
+        buffers, valid until its next call."""
         t = self.torch
         n = len(feats)
         self._reserve(n)
-        s = t.cuda.current_stream()
-        self.h_feats[:n].numpy()[:] = feats
-        self.d_feats[:n].copy_(self.h_feats[:n], non_blocking=True)
-        self.launch(self.d_feats, n, self.d_out, self.d_rd, self.d_spread, self.d_route, s.cuda_stream)
-        self.h_out[:n].copy_(self.d_out[:n], non_blocking=True)
-        self.h_rd[:n].copy_(self.d_rd[:n], non_blocking=True)
-        self.h_route[:n].copy_(self.d_route[:n], non_blocking=True)
-        if spreads is not None:
-            self.h_spread[:n].copy_(self.d_spread[:n], non_blocking=True)
-        s.synchronize()
+        if isinstance(feats, t.Tensor) and feats.is_pinned() and feats.dtype == t.float32:
+            src = feats
+        else:
+            self.h_feats[:n].numpy()[:] = feats
+            src = self.h_feats
+        if not hasattr(self, "streams"):
+            self.streams = [t.cuda.Stream(device=self.ens.dev) for _ in range(2)]
+        cur = t.cuda.current_stream()
+        for st in self.streams:
+            st.wait_stream(cur)
+        for i, a in enumerate(range(0, n, chunk)):
+            b = min(n, a + chunk)
+            st = self.streams[i % 2]
+            with t.cuda.stream(st):
+                self.d_feats[a:b].copy_(src[a:b], non_blocking=True)
+                self.launch(self.d_feats[a:b], b - a, self.d_out[a:b], self.d_rd[a:b], self.d_spread[a:b],
+                            self.d_route[a:b], st.cuda_stream)
+                self.h_out[a:b].copy_(self.d_out[a:b], non_blocking=True)
+                self.h_rd[a:b].copy_(self.d_rd[a:b], non_blocking=True)
+                self.h_route[a:b].copy_(self.d_route[a:b], non_blocking=True)
+                if spreads is not None:
+                    self.h_spread[a:b].copy_(self.d_spread[a:b], non_blocking=True)
+        for st in self.streams:
+            st.synchronize()
         if lib().tmc_b200_nn_status(1):
             raise RuntimeError("a tensor-core wait gave up in the fused ensemble kernel")
         if spreads is not None:
             spreads.append(self.h_spread[:n].numpy().copy())
-        return (self.h_out[:n].numpy().astype(np.float64), self.h_rd[:n].numpy().copy(),
-                self.h_route[:n].numpy().astype(bool))
+        y, rd, route = self.h_out[:n].numpy(), self.h_rd[:n].numpy(), self.h_route[:n].numpy().view(bool)
+        return (y.copy(), rd.copy(), route.copy()) if copy else (y, rd, route)
 
 
 def spread(members_out: np.ndarray) -> np.ndarray:
