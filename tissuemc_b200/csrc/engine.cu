@@ -255,6 +255,13 @@ WalkParams make_params(const tmc_run_spec &spec, const tmc_options &opt, const P
     // ids a warp claims at once: one per lane, so that when the ids run out no warp is left holding
     // a backlog of unstarted photons while others idle
     P.chunk = 32;
+    uint32_t k0 = static_cast<uint32_t>(opt.seed), k1 = static_cast<uint32_t>(opt.seed >> 32);
+    for (int r = 0; r < 10; ++r) {  // Philox4x32 key schedule (Weyl increments)
+        P.round_keys[2 * r] = k0;
+        P.round_keys[2 * r + 1] = k1;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
     fill_layers(spec, P.layers);
     return P;
 }

@@ -79,7 +79,7 @@ template <int FAST> struct SweepCtx {
     }
     __device__ __forceinline__ void absorb(const Lane &L, unsigned long long v) {
         if (!P.profiles) return;
-        const float rr = m_sqrt<FAST>(L.x * L.x + L.y * L.y);
+        const float rr = radius<FAST>(L.x, L.y);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int iz = bin_of<FAST>(L.z, P.dz, P.inv_dz, P.nz);
         const int key = static_cast<int>(t - P.tally) + a_off + ir * P.nz + iz;
@@ -97,7 +97,7 @@ template <int FAST> struct SweepCtx {
     }
     __device__ __forceinline__ void exit(const Lane &L, int kind, unsigned long long v) const {
         if (!P.profiles) return;
-        const float rr = m_sqrt<FAST>(L.x * L.x + L.y * L.y);
+        const float rr = radius<FAST>(L.x, L.y);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int ia = P.na > 1 ? bin_of<FAST>(acosf(fminf(fabsf(L.uz), 1.0f)), P.da, P.inv_da, P.na) : 0;
         atomicAdd(&t[(kind == 1 ? rd_off : tt_off) + ir * P.na + ia], v);
@@ -105,11 +105,11 @@ template <int FAST> struct SweepCtx {
 };
 
 // Minimum resident 256-thread blocks per SM the compiler must allow for (0: no bound). A bound of
-// 4 caps the kernel at 64 registers and runs 2.3 % faster, but the tighter register budget changes
-// which multiply-adds the code generator fuses, so its tallies stop being bit-identical to the
-// single-run kernel's; the default keeps them identical.
+// 4 caps the kernel at 64 registers (four blocks per SM instead of three). The step's arithmetic has
+// its rounding pinned (walk.cuh), so the register budget cannot change any photon's path: the
+// tallies stay bit-identical to the single-run kernel's.
 #ifndef TMC_SWEEP_MIN_BLOCKS
-#define TMC_SWEEP_MIN_BLOCKS 0
+#define TMC_SWEEP_MIN_BLOCKS 4
 #endif
 #if TMC_SWEEP_MIN_BLOCKS > 0
 #define TMC_SWEEP_BOUNDS __launch_bounds__(256, TMC_SWEEP_MIN_BLOCKS)

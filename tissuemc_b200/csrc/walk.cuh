@@ -65,6 +65,8 @@ struct WalkParams {
     int profiles;          // 0: skip A(r,z), R_d(r,a), T_t(r,a)
     uint32_t step_cap;     // a packet still alive after this many steps is ended as an anomaly
     int chunk;             // photon ids claimed per warp refill (>= 32)
+    uint32_t round_keys[20];  // Philox key schedule of `seed` (k0, k1 of rounds 0..9), so that the
+                              // rounds read their keys from the parameter bank instead of adding
     LayerC layers[kMaxLayers];
 };
 
@@ -85,6 +87,27 @@ __device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t
         c3 = static_cast<uint32_t>(p0);
         k0 += 0x9E3779B9u;
         k1 += 0xBB67AE85u;
+    }
+    o0 = c0;
+    o1 = c1;
+    o2 = c2;
+    o3 = c3;
+}
+
+// The same rounds with the key schedule given (round r uses rk[2r], rk[2r + 1]).
+__device__ __forceinline__ void philox4x32_10_rk(uint32_t c0, uint32_t c1, uint32_t c2, const uint32_t (&rk)[20],
+                                                 uint32_t &o0, uint32_t &o1, uint32_t &o2, uint32_t &o3) {
+    uint32_t c3 = 0u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * c0;
+        const uint64_t p1 = static_cast<uint64_t>(0xCD9E8D57u) * c2;
+        const uint32_t n0 = static_cast<uint32_t>(p1 >> 32) ^ c1 ^ rk[2 * r];
+        const uint32_t n2 = static_cast<uint32_t>(p0 >> 32) ^ c3 ^ rk[2 * r + 1];
+        c0 = n0;
+        c1 = static_cast<uint32_t>(p1);
+        c2 = n2;
+        c3 = static_cast<uint32_t>(p0);
     }
     o0 = c0;
     o1 = c1;
@@ -139,8 +162,21 @@ template <int MODE> __device__ __forceinline__ float m_log(float x) {
     else return logf(x);
 }
 
+// The step's floating-point arithmetic is written with its rounding pinned: every product, sum and
+// fused multiply-add is an explicit round-to-nearest intrinsic, which the compiler may not contract
+// or split. Two kernels that share the step (the single run and the sweep) therefore compute every
+// photon identically whatever their register budgets, and the sweep's tallies stay bit for bit those
+// of single runs.
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+// a^2 + b^2 + c^2 and a^2 + b^2
+__device__ __forceinline__ float norm2(float a, float b, float c) { return ffma(a, a, ffma(b, b, fmul(c, c))); }
+__device__ __forceinline__ float norm2(float a, float b) { return ffma(a, a, fmul(b, b)); }
+
 __device__ __forceinline__ unsigned long long to_fixed(float w) {
-    return __float2ull_rn(w * kFixedScale);
+    return __float2ull_rn(fmul(w, kFixedScale));
 }
 
 

@@ -45,8 +45,7 @@ __host__ __device__ inline SmemLayout smem_layout(const WalkParams &P) {
 // one-entry run cache of A(r,z) deposits per lane.
 template <int FAST> struct PlainCtx {
     const WalkParams &P;
-    Ring ring;
-    uint32_t k0, k1;
+    Ring ring;  // refilled with the launch's precomputed Philox key schedule (P.round_keys)
     uint32_t step_cap;
     const LayerC *layers;
     unsigned long long *bt;
@@ -56,7 +55,7 @@ template <int FAST> struct PlainCtx {
     int cache_ir, cache_iz;  // the run cache outlives photons; flushed at the end
     unsigned long long cache_val;
 
-    __device__ __forceinline__ void refill(Lane &L) const { ring.refill(L, k0, k1); }
+    __device__ __forceinline__ void refill(Lane &L) const { ring.refill(L, P.round_keys); }
     __device__ __forceinline__ uint32_t draw(Lane &L) const { return ring.draw(L); }
     __device__ __forceinline__ const LayerC &layer(const Lane &, int l) const { return layers[l]; }
     __device__ __forceinline__ int num_layers(const Lane &) const { return P.nl; }
@@ -79,7 +78,7 @@ template <int FAST> struct PlainCtx {
 
     __device__ __forceinline__ void absorb(const Lane &L, unsigned long long v) {
         if (!P.profiles) return;
-        const float rr = m_sqrt<FAST>(L.x * L.x + L.y * L.y);
+        const float rr = radius<FAST>(L.x, L.y);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int iz = bin_of<FAST>(L.z, P.dz, P.inv_dz, P.nz);
         if (ir == cache_ir && iz == cache_iz) {
@@ -99,7 +98,7 @@ template <int FAST> struct PlainCtx {
 
     __device__ __forceinline__ void exit(const Lane &L, int kind, unsigned long long v) const {
         if (!P.profiles) return;
-        const float rr = m_sqrt<FAST>(L.x * L.x + L.y * L.y);
+        const float rr = radius<FAST>(L.x, L.y);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int ia = bin_of<FAST>(acosf(fminf(fabsf(L.uz), 1.0f)), P.da, P.inv_da, P.na);
         if (kind == 1) {
@@ -136,8 +135,6 @@ __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P
     __syncthreads();
     PlainCtx<FAST> C{P,
                      Ring{reinterpret_cast<uint32_t *>(smem + S.ring) + threadIdx.x, static_cast<int>(P.threads)},
-                     static_cast<uint32_t>(P.seed),
-                     static_cast<uint32_t>(P.seed >> 32),
                      P.step_cap,
                      reinterpret_cast<const LayerC *>(smem + S.layers),
                      P.batch_smem ? smem + S.batch : P.g_batch,

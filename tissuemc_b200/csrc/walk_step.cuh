@@ -62,30 +62,31 @@ __device__ __forceinline__ float fresnel(float n1, float n2, float ca1, float rn
         ca2 = 0.0f;
         return 1.0f;
     }
-    const float sa1 = m_sqrt<FAST>(1.0f - ca1 * ca1);
+    const float sa1 = m_sqrt<FAST>(ffma(-ca1, ca1, 1.0f));
     float sa2;
-    if constexpr (Math<FAST>::div) sa2 = sa1 * rat;
-    else sa2 = n1 * sa1 / n2;
+    if constexpr (Math<FAST>::div) sa2 = fmul(sa1, rat);
+    else sa2 = fmul(n1, sa1) / n2;
     if (sa2 >= 1.0f) {
         ca2 = 0.0f;
         return 1.0f;
     }
-    ca2 = m_sqrt<FAST>(1.0f - sa2 * sa2);
-    const float cap = ca1 * ca2 - sa1 * sa2;
-    const float cam = ca1 * ca2 + sa1 * sa2;
-    const float sap = sa1 * ca2 + ca1 * sa2;
-    const float sam = sa1 * ca2 - ca1 * sa2;
-    return m_div<FAST>(0.5f * sam * sam * (cam * cam + cap * cap), sap * sap * cam * cam);
+    ca2 = m_sqrt<FAST>(ffma(-sa2, sa2, 1.0f));
+    const float cc = fmul(ca1, ca2), ss = fmul(sa1, sa2), sc = fmul(sa1, ca2), cs = fmul(ca1, sa2);
+    const float cap = fsub(cc, ss), cam = fadd(cc, ss), sap = fadd(sc, cs), sam = fsub(sc, cs);
+    return m_div<FAST>(fmul(fmul(fmul(0.5f, sam), sam), norm2(cam, cap)), fmul(fmul(sap, sap), fmul(cam, cam)));
 }
 
 // Clamped bin index (src/cpu/engine.cpp:59-66 semantics, branch-free): x <= 0 or NaN -> 0,
 // x / width >= n -> n - 1, else floor(x / width).
 template <int FAST> __device__ __forceinline__ int bin_of(float x, float width, float inv_width, int n) {
     float i;
-    if constexpr (Math<FAST>::div) i = x * inv_width;
+    if constexpr (Math<FAST>::div) i = fmul(x, inv_width);
     else i = x / width;
     return static_cast<int>(fminf(fmaxf(i, 0.0f), static_cast<float>(n - 1)));
 }
+
+// Radial distance of the packet from the source axis (the r of A(r,z), R_d(r,a), T_t(r,a)).
+template <int FAST> __device__ __forceinline__ float radius(float x, float y) { return m_sqrt<FAST>(norm2(x, y)); }
 
 // All state of one lane's current photon (registers).
 struct Lane {
@@ -126,29 +127,29 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
         if constexpr (Math<FAST>::log) {
             // the SFU logarithm's absolute error can flip the sign of log(u) for the two largest
             // u of the 23-bit grid; a step is never negative
-            s = fmaxf(-m_log<FAST>(u), 0.0f) * L.h.inv_mut;
+            s = fmul(fmaxf(-m_log<FAST>(u), 0.0f), L.h.inv_mut);
         } else if constexpr (Math<FAST>::div) {
-            s = -m_log<FAST>(u) * L.h.inv_mut;
+            s = fmul(-m_log<FAST>(u), L.h.inv_mut);
         } else {
             s = -m_log<FAST>(u) / L.h.mut;
         }
     } else {
-        if constexpr (Math<FAST>::div) s = L.sleft * L.h.inv_mut;
+        if constexpr (Math<FAST>::div) s = fmul(L.sleft, L.h.inv_mut);
         else s = L.sleft / L.h.mut;
         L.sleft = 0.0f;
     }
     bool hit = false;
     if (L.uz != 0.0f) {
-        const float db = m_div<FAST>((L.uz > 0.0f ? L.h.z1 : L.h.z0) - L.z, L.uz);
+        const float db = m_div<FAST>(fsub(L.uz > 0.0f ? L.h.z1 : L.h.z0, L.z), L.uz);
         if (s > db) {
-            L.sleft = (s - db) * L.h.mut;
+            L.sleft = fmul(fsub(s, db), L.h.mut);
             s = db;
             hit = true;
         }
     }
-    L.x += s * L.ux;
-    L.y += s * L.uy;
-    L.z += s * L.uz;
+    L.x = ffma(s, L.ux, L.x);
+    L.y = ffma(s, L.uy, L.y);
+    L.z = ffma(s, L.uz, L.z);
 
     bool died = false;
     int exit_kind = 0;  // 1: reflectance (top), 2: transmittance (bottom)
@@ -164,8 +165,8 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
                             ? 1.0f
                             : fresnel<FAST>(Lc.n, nt, ca1, up ? Lc.rn_up : Lc.rn_dn, rat, uz1);
         if (unit_open(C.draw(L)) > r) {
-            L.ux *= rat;
-            L.uy *= rat;
+            L.ux = fmul(L.ux, rat);
+            L.uy = fmul(L.uy, rat);
             L.uz = up ? -uz1 : uz1;
             if (up ? L.layer == 0 : L.layer == C.num_layers(L) - 1) {
                 exit_kind = up ? 1 : 2;
@@ -184,13 +185,13 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
     } else {
         // ---- drop (physics.hpp:187-193) and score the absorption
         float dwa;
-        if constexpr (Math<FAST>::div) dwa = L.w * L.h.absorb;
-        else dwa = L.w * L.h.mua / L.h.mut;
-        L.w -= dwa;
+        if constexpr (Math<FAST>::div) dwa = fmul(L.w, L.h.absorb);
+        else dwa = fmul(L.w, L.h.mua) / L.h.mut;
+        L.w = fsub(L.w, dwa);
         ++L.events;
         {
-            const float n2 = L.ux * L.ux + L.uy * L.uy + L.uz * L.uz;
-            if (!(dwa == dwa) || !(fabsf(n2 - 1.0f) <= 1e-5f)) ++L.anomalies;
+            const float n2 = norm2(L.ux, L.uy, L.uz);
+            if (!(dwa == dwa) || !(fabsf(fsub(n2, 1.0f)) <= 1e-5f)) ++L.anomalies;
         }
         const unsigned long long v = to_fixed(dwa);
         L.run_abs += v;
@@ -200,56 +201,59 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
         {
             const float xi = unit_open(C.draw(L));
             if (L.h.g == 0.0f) {
-                ct = 2.0f * xi - 1.0f;
+                ct = ffma(2.0f, xi, -1.0f);
             } else {
-                const float t = m_div<FAST>(L.h.hg_a, L.h.hg_b + L.h.hg_c * xi);
-                if constexpr (Math<FAST>::div) ct = (L.h.hg_d - t * t) * L.h.inv_2g;
-                else ct = (L.h.hg_d - t * t) / L.h.hg_c;
+                const float t = m_div<FAST>(L.h.hg_a, ffma(L.h.hg_c, xi, L.h.hg_b));
+                if constexpr (Math<FAST>::div) ct = fmul(ffma(-t, t, L.h.hg_d), L.h.inv_2g);
+                else ct = ffma(-t, t, L.h.hg_d) / L.h.hg_c;
                 ct = fminf(fmaxf(ct, -1.0f), 1.0f);
             }
         }
-        float st = 1.0f - ct * ct;
+        float st = ffma(-ct, ct, 1.0f);
         st = st > 0.0f ? m_sqrt<FAST>(st) : 0.0f;
         float sp, cp;
         {
             const float u = unit_open(C.draw(L));
             if constexpr (Math<FAST>::sincos) {
                 // psi - pi lies in (-pi, pi), where the SFU sine and cosine are accurate
-                __sincosf(kTwoPi * (u - 0.5f), &sp, &cp);
+                __sincosf(fmul(kTwoPi, fsub(u, 0.5f)), &sp, &cp);
                 sp = -sp;
                 cp = -cp;
             } else {
-                sincosf(kTwoPi * u, &sp, &cp);
+                sincosf(fmul(kTwoPi, u), &sp, &cp);
             }
         }
         if (fabsf(L.uz) > kCosZero) {
-            L.ux = st * cp;
-            L.uy = st * sp;
+            L.ux = fmul(st, cp);
+            L.uy = fmul(st, sp);
             L.uz = L.uz >= 0.0f ? ct : -ct;
         } else {
             const float ox = L.ux, oy = L.uy, oz = L.uz;
+            const float q = ffma(-oz, oz, 1.0f);  // 1 - uz^2
+            const float ix = ffma(fmul(ox, oz), cp, -fmul(oy, sp));
+            const float iy = ffma(fmul(oy, oz), cp, fmul(ox, sp));
             if constexpr (Math<FAST>::sqrt) {
-                const float it = rsqrtf(1.0f - oz * oz);
-                L.ux = st * (ox * oz * cp - oy * sp) * it + ox * ct;
-                L.uy = st * (oy * oz * cp + ox * sp) * it + oy * ct;
-                L.uz = -st * cp * (1.0f - oz * oz) * it + oz * ct;
+                const float it = rsqrtf(q);
+                L.ux = ffma(fmul(st, ix), it, fmul(ox, ct));
+                L.uy = ffma(fmul(st, iy), it, fmul(oy, ct));
+                L.uz = ffma(fmul(fmul(-st, cp), q), it, fmul(oz, ct));
             } else {
-                const float tmp = sqrtf(1.0f - oz * oz);
-                L.ux = st * (ox * oz * cp - oy * sp) / tmp + ox * ct;
-                L.uy = st * (oy * oz * cp + ox * sp) / tmp + oy * ct;
-                L.uz = -st * cp * tmp + oz * ct;
+                const float tmp = sqrtf(q);
+                L.ux = fadd(fmul(st, ix) / tmp, fmul(ox, ct));
+                L.uy = fadd(fmul(st, iy) / tmp, fmul(oy, ct));
+                L.uz = ffma(fmul(-st, cp), tmp, fmul(oz, ct));
             }
         }
-        const float inv = m_rsqrt<FAST>(L.ux * L.ux + L.uy * L.uy + L.uz * L.uz);
-        L.ux *= inv;
-        L.uy *= inv;
-        L.uz *= inv;
+        const float inv = m_rsqrt<FAST>(norm2(L.ux, L.uy, L.uz));
+        L.ux = fmul(L.ux, inv);
+        L.uy = fmul(L.uy, inv);
+        L.uz = fmul(L.uz, inv);
     }
 
     if (exit_kind) {
         // ---- score the exit (check, totals, R_d(r,a) or T_t(r,a))
-        const float n2 = L.ux * L.ux + L.uy * L.uy + L.uz * L.uz;
-        if (!(L.w == L.w) || !(fabsf(n2 - 1.0f) <= 1e-5f)) ++L.anomalies;
+        const float n2 = norm2(L.ux, L.uy, L.uz);
+        if (!(L.w == L.w) || !(fabsf(fsub(n2, 1.0f)) <= 1e-5f)) ++L.anomalies;
         const unsigned long long v = to_fixed(L.w);
         C.batch_add(L, exit_kind - 1, v);
         C.exit(L, exit_kind, v);
@@ -258,7 +262,7 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
         if (L.w == 0.0f) {
             died = true;
         } else if (unit_open(C.draw(L)) < kChance) {
-            if constexpr (Math<FAST>::div) L.w *= 10.0f;
+            if constexpr (Math<FAST>::div) L.w = fmul(L.w, 10.0f);
             else L.w /= kChance;
         } else {
             died = true;
@@ -287,9 +291,7 @@ struct Ring {
         ++L.rp;
         return o;
     }
-    __device__ __forceinline__ void refill(Lane &L, uint32_t k0, uint32_t k1) const {
-        uint32_t b0, b1, b2, b3;
-        philox4x32_10(L.id, 0u, L.blk, k0, k1, b0, b1, b2, b3);
+    __device__ __forceinline__ void store(Lane &L, uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3) const {
         ++L.blk;
         uint32_t *const slot = base + (L.wp & 4u) * stride;  // wp is a multiple of 4
         slot[0] = b0;
@@ -297,6 +299,17 @@ struct Ring {
         slot[2 * stride] = b2;
         slot[3 * stride] = b3;
         L.wp += 4u;
+    }
+    __device__ __forceinline__ void refill(Lane &L, uint32_t k0, uint32_t k1) const {
+        uint32_t b0, b1, b2, b3;
+        philox4x32_10(L.id, 0u, L.blk, k0, k1, b0, b1, b2, b3);
+        store(L, b0, b1, b2, b3);
+    }
+    // with a precomputed key schedule (one key for every lane of the launch)
+    __device__ __forceinline__ void refill(Lane &L, const uint32_t (&rk)[20]) const {
+        uint32_t b0, b1, b2, b3;
+        philox4x32_10_rk(L.id, 0u, L.blk, rk, b0, b1, b2, b3);
+        store(L, b0, b1, b2, b3);
     }
 };
 
