@@ -24,7 +24,7 @@ def pytest_configure(config):
 def _built():
     from tissuemc_b200 import build as b
 
-    if not b.LIB.exists() or not b.CLI.exists():
+    if not b.LIB.exists() or not b.CLI.exists() or not b.DIGEST.exists():
         b.build()
     if not (ROOT / "oracle" / "liboracle.so").exists():
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), str(ROOT / "oracle" / "liboracle.so")],

@@ -21,6 +21,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libtissuemc_b200.so"
 CLI = PKG / "bin" / "tissuemc"
+DIGEST = PKG / "bin" / "ncu_digest"  # Nsight Compute CSV digest (host tool, no CUDA)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
@@ -88,6 +89,9 @@ def build(verbose: bool = False) -> Path:
     if _stale(CLI, [*cli_srcs, LIB, *hdrs]):
         _run([cxx, *[f for f in CXX_FLAGS if f != "-fvisibility=hidden"], *map(str, cli_srcs), "-o", str(CLI),
               f"-L{PKG}", "-ltissuemc_b200", "-Wl,-rpath,$ORIGIN/..", "-pthread"])
+    dsrc = CSRC / "host" / "ncu_digest.cpp"
+    if _stale(DIGEST, [dsrc]):
+        _run([cxx, *[f for f in CXX_FLAGS if f != "-fvisibility=hidden"], str(dsrc), "-o", str(DIGEST)])
     return LIB
 
 
