@@ -273,3 +273,25 @@ def test_bad_device_ordinal_is_no_device(slab):
     with pytest.raises(tmc.EngineError) as e:
         tmc.run(slab, photons=100, batches=1, device=63)
     assert e.value.code == tmc.NO_DEVICE
+
+
+REF_CUDA = oracle.REF_BIN.parent / "tissuemc_cuda"
+
+
+@pytest.mark.skipif(not REF_CUDA.exists(),
+                    reason="the reference's CUDA engine is not built here (make -C oracle ref_cuda)")
+@pytest.mark.parametrize("rung", [7, 8])
+def test_slab_identical_photons_vs_the_reference_cuda_engine(slab, slab_gpu, tmp_path, rung):
+    """The reference's own GPU engine (its rungs 7 and 8, float32 transport) on the same device,
+    same seed and batches: the reference's identical-photon limits on totals, per batch, events,
+    a_z and rd_r."""
+    import json
+    import subprocess
+
+    out = tmp_path / "ref.json"
+    p = subprocess.run([str(REF_CUDA), "run", str(tmc.CONFIGS / "slab_n14.mci"), "--engine", "cuda", "--rung",
+                        str(rung), "--photons", "1000000", "--batches", "80", "--seed", "1", "--output", str(out)],
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    ref = from_reference_json(json.loads(out.read_text())["runs"][0])
+    _assert_gaps(identical_photon_gaps(ref, from_engine(slab_gpu), profiles=("a_z", "rd_r")))
