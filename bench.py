@@ -69,7 +69,7 @@ def _args():
                     help="override the workload's photon count (for profiling captures only)")
     ap.add_argument("--autotune", action="store_true", help="sweep: pick the launch shape first")
     ap.add_argument("--scale", type=float, default=1.0, help="surrogate: fraction of the full data and query counts")
-    ap.add_argument("--epochs", type=int, default=20, help="surrogate: training epochs")
+    ap.add_argument("--epochs", type=int, default=300, help="surrogate: training epochs")
     ap.add_argument("--queries", type=int, default=1 << 20, help="serve: queries per step")
     ap.add_argument("--configs", type=int, default=4096, help="sweep: configurations")
     ap.add_argument("--photon-scale", type=float, default=1.0, help="sweep: scale every configuration's photons "

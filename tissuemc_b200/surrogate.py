@@ -568,7 +568,7 @@ def pipeline(scale: float = 1.0, members: int = 4, epochs: int = 20, seed: int =
 
     t0 = time.perf_counter()
     ens = Ensemble(members=members, batch=4096, seed=seed)
-    hist = ens.train(X, Y, epochs=epochs, lr=2e-3)
+    hist = ens.train(X, Y, epochs=epochs, lr=1e-3, ema=0.999)
     torch.cuda.synchronize()
     out["train"] = {"seconds": time.perf_counter() - t0, "loss_first": hist[0], "loss_last": hist[-1]}
     ph = ens.predict(Xh)
@@ -587,10 +587,13 @@ def pipeline(scale: float = 1.0, members: int = 4, epochs: int = 20, seed: int =
     pred_rd = rd_profile(ens.predict(Xh[:n_acc]))
     counted = ref[:, :N_RD] * acc_photons >= 1e4  # bins with at least ~1e4 photons of signal
     rel = np.abs(pred_rd - ref_rd) / np.maximum(ref_rd, 1e-30)
+    # the profile's relative L2 error over the counted bins, per configuration
+    l2 = np.sqrt((((pred_rd - ref_rd) * counted) ** 2).sum(1) / ((ref_rd * counted) ** 2).sum(1))
     out["accuracy_vs_mc"] = {"configs": n_acc, "mc_photons": acc_photons, "bins": int(counted.sum()),
                              "median_rel_err": float(np.median(rel[counted])),
                              "p90_rel_err": float(np.quantile(rel[counted], 0.9)),
-                             "frac_bins_within_1pct": float((rel[counted] <= 0.01).mean())}
+                             "frac_bins_within_1pct": float((rel[counted] <= 0.01).mean()),
+                             "profile_l2_median": float(np.median(l2)), "profile_l2_p90": float(np.quantile(l2, 0.9))}
     log(f"accuracy: {out['accuracy_vs_mc']}")
 
     # gated serving
@@ -614,6 +617,19 @@ def pipeline(scale: float = 1.0, members: int = 4, epochs: int = 20, seed: int =
         out["accuracy_vs_mc"]["kept_by_gate"] = int(keep.sum())
         out["accuracy_vs_mc"]["kept_median_rel_err"] = float(np.median(rel[keep][counted[keep]]))
         out["accuracy_vs_mc"]["kept_frac_bins_within_1pct"] = float((rel[keep][counted[keep]] <= 0.01).mean())
+        out["accuracy_vs_mc"]["kept_profile_l2_median"] = float(np.median(l2[keep]))
+    # the gated answers (network where the gate keeps the query, 1e6-photon MC where it routes it)
+    mc6 = (CSweepConfig * n_acc)(*hcfg[:n_acc])
+    for c in mc6:
+        c.photons = 1_000_000
+    mc6_rd = sweep_run(mc6, sweep_options()).summary[:, :N_RD] / areas
+    ans = np.where(keep[:, None], pred_rd, mc6_rd)
+    rel_g = np.abs(ans - ref_rd) / np.maximum(ref_rd, 1e-30)
+    l2_g = np.sqrt((((ans - ref_rd) * counted) ** 2).sum(1) / ((ref_rd * counted) ** 2).sum(1))
+    rel_mc = np.abs(mc6_rd - ref_rd) / np.maximum(ref_rd, 1e-30)
+    out["accuracy_vs_mc"]["gated_median_rel_err"] = float(np.median(rel_g[counted]))
+    out["accuracy_vs_mc"]["gated_profile_l2_median"] = float(np.median(l2_g))
+    out["accuracy_vs_mc"]["plain_mc_1e6_median_rel_err"] = float(np.median(rel_mc[counted]))
     idx = np.flatnonzero(routed)
     t_mc, simulated = 0.0, 0
     if len(idx):
@@ -640,7 +656,12 @@ def pipeline(scale: float = 1.0, members: int = 4, epochs: int = 20, seed: int =
                       "routed_simulated": simulated,
                       "network_seconds": t_net, "mc_seconds": t_mc, "gated_queries_per_s": gated_rate,
                       "network_queries_per_s": n_q / t_net, "plain_mc_solves_per_s_1e6_photons": mc_rate,
-                      "speedup_vs_plain_mc": gated_rate / mc_rate}
+                      "speedup_vs_plain_mc": gated_rate / mc_rate,
+                      # the same measured network and MC times, with the routed fraction of other
+                      # gate thresholds (projected, not re-run)
+                      "projected_speedup_vs_threshold": {
+                          f"{th:g}": n_q / (t_net + float((sp > th).sum()) / mc_rate) / mc_rate
+                          for th in (0.005, 0.01, 0.02, 0.05)}}
     log(f"serving: {out['serving']}")
 
     # inverse fits of two-layer tissues
