@@ -136,6 +136,13 @@ def test_run_device_then_decode_equals_run(slab):
 
 
 # ---------------------------------------------------------------- edge cases and other media
+# Photons for the edge-case identical-photon tests. A float32 last-bit difference (SFU functions,
+# fused multiply-adds) now and then sends one packet down another path; the reference's profile-total
+# limit (1e-4 relative) is meant for full-size runs, and at 1e5 photons it tolerates only two or three
+# such packets. The expected gap shrinks as 1/sqrt(photons), so these runs use 3e5.
+EDGE_PHOTONS = 300_000
+
+
 def _parity(spec: tmc.RunSpec, photons: int, batches: int, seed: int, profiles=("a_z", "rd_r", "tt_r")):
     g = tmc.run(spec, photons=photons, batches=batches, seed=seed)
     o = oracle.run(_ospec(spec), photons, batches, seed, 32, threads=0)
@@ -155,7 +162,7 @@ def test_single_photon_and_one_photon_per_batch(slab):
 def test_single_bin_grid():
     spec = tmc.RunSpec(layers=[(1.37, 1, 100, 0.9, 0.1), (1.37, 1, 10, 0, 0.1), (1.37, 2, 10, 0.7, 0.2)],
                        dz=0.01, dr=0.01, nz=1, nr=1, na=1)
-    g, o, gaps = _parity(spec, 100_000, 10, 1)
+    g, o, gaps = _parity(spec, EDGE_PHOTONS, 10, 1)
     _assert_gaps(gaps)
     assert math.isclose(g.a_rz[0, 0], g.absorbed.sum(), rel_tol=1e-12)
 
@@ -163,14 +170,14 @@ def test_single_bin_grid():
 def test_sixteen_layers_with_mismatched_indices():
     layers = [(1.3 + 0.02 * i, 0.5 + 0.1 * i, 50 + 5 * i, 0.5 + 0.02 * i, 0.01 + 0.002 * i) for i in range(16)]
     spec = tmc.RunSpec(layers=layers, dz=0.01, dr=0.01, nz=40, nr=40, na=5, n_above=1.0, n_below=1.2)
-    _, _, gaps = _parity(spec, 100_000, 10, 8)
+    _, _, gaps = _parity(spec, EDGE_PHOTONS, 10, 8)
     _assert_gaps(gaps)
 
 
 @pytest.mark.parametrize("g_aniso", [0.0, -0.3, 0.95])
 def test_anisotropy_extremes(g_aniso):
     spec = tmc.RunSpec(layers=[(1.5, 2, 50, g_aniso, 0.05)], dz=0.005, dr=0.005, nz=20, nr=40, na=10)
-    _, _, gaps = _parity(spec, 100_000, 10, 21)
+    _, _, gaps = _parity(spec, EDGE_PHOTONS, 10, 21)
     _assert_gaps(gaps)
 
 
