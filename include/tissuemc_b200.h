@@ -293,6 +293,9 @@ TMC_B200_API int tmc_b200_gemm_bf16(const uint16_t *A, const uint16_t *B, const 
  *                weight, N = the layer's inputs), Zprev: M x N.
  * matmul_f32:    D = A B^T (float32); A: M x K, B: N x K (weight gradients from transposed
  *                activations).
+ * matmul_f32_splitk: the same with K cut into `splits` equal ranges computed by separate CTAs
+ *                (K / 64 a multiple of splits) into work (splits x M x N floats), then summed into
+ *                D in a fixed order (deterministic); for long K and small M x N.
  * transpose:     Y = X^T for a rows x cols bf16 matrix.
  * colsum:        db[n] = sum_m dZ[m][n] (float32, overwritten).
  * mse:           loss += scale * sum (pred - target)^2 over the first T of ld columns; dZ (bf16,
@@ -308,6 +311,9 @@ TMC_B200_API int tmc_b200_nn_backward_data(const uint16_t *dZ, const uint16_t *W
                                            int32_t M, int32_t N, int32_t K, void *stream, tmc_status *status);
 TMC_B200_API int tmc_b200_nn_matmul_f32(const uint16_t *A, const uint16_t *B, float *D, int32_t M, int32_t N,
                                         int32_t K, void *stream, tmc_status *status);
+TMC_B200_API int tmc_b200_nn_matmul_f32_splitk(const uint16_t *A, const uint16_t *B, float *D, float *work,
+                                               int32_t M, int32_t N, int32_t K, int32_t splits, void *stream,
+                                               tmc_status *status);
 TMC_B200_API int tmc_b200_nn_transpose(const uint16_t *X, uint16_t *Y, int32_t rows, int32_t cols, void *stream,
                                        tmc_status *status);
 TMC_B200_API int tmc_b200_nn_colsum(const uint16_t *dZ, float *db, int32_t M, int32_t N, void *stream,

@@ -31,6 +31,27 @@ def test_tensor_core_gemm_matches_fp32_reference(M, N, K):
     assert rel < 2e-6, rel  # FP32 accumulation of exact BF16 products
 
 
+@pytest.mark.parametrize("M,N,K,splits", [(512, 512, 4096, 8), (130, 72, 192, 3), (128, 128, 64, 1)])
+def test_split_k_weight_gradient_product(M, N, K, splits):
+    """D = A B^T with K cut into splits (the weight-gradient shape: long K, small M x N)."""
+    import ctypes
+
+    from tissuemc_b200 import surrogate as S
+
+    g = torch.Generator(device="cuda").manual_seed(K + splits)
+    A = torch.randn(M, K, device="cuda", generator=g).bfloat16()
+    B = torch.randn(N, K, device="cuda", generator=g).bfloat16()
+    D = torch.empty(M, N, device="cuda")
+    work = torch.empty(splits * M * N, device="cuda")
+    S._call("tmc_b200_nn_matmul_f32_splitk", S._p(A), S._p(B), S._p(D), S._p(work), M, N, K, splits,
+            ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    ref = A.double() @ B.double().T
+    assert ((D.double() - ref).abs().max() / ref.abs().max()).item() < 2e-6
+    with pytest.raises(tmc.ConfigError, match="split-K"):
+        S._call("tmc_b200_nn_matmul_f32_splitk", S._p(A), S._p(B), S._p(D), S._p(work), M, N, K, 5,
+                ctypes.c_void_p(0))
+
+
 def test_gemm_rejects_k_not_multiple_of_64():
     A = torch.zeros(128, 32, device="cuda", dtype=torch.bfloat16)
     with pytest.raises(tmc.ConfigError, match="multiple of 64"):

@@ -23,20 +23,23 @@ namespace tmc {
 namespace {
 
 constexpr int kBN = 128;
-constexpr int kGemmSmemRequest = 60 * 1024;  // at most three CTAs per SM: 3 x 128 of 512 TMEM columns
+// two stages of 32 KB plus slack: at most three CTAs per SM, i.e. 3 x 128 of the 512 TMEM columns
+constexpr int kGemmSmemRequest = 68 * 1024;
+static_assert(GemmSmem<128>::bytes <= kGemmSmemRequest, "GEMM shared memory");
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float x) {
     return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
 }
 
-// D (float32) = acc (+ bias)
+// D (float32) = acc (+ bias); split z of a split-K product writes its partial at D + z * split_stride
 struct EpiF32 {
     float *D;
     const float *bias;
     int N;
-    __device__ __forceinline__ void operator()(int row, int col, const float (&v)[8]) const {
-        float *d = D + static_cast<size_t>(row) * N + col;
+    size_t split_stride;
+    __device__ __forceinline__ void operator()(int split, int row, int col, const float (&v)[8]) const {
+        float *d = D + split * split_stride + static_cast<size_t>(row) * N + col;
 #pragma unroll
         for (int i = 0; i < 8; ++i)
             if (col + i < N) d[i] = v[i] + (bias ? bias[col + i] : 0.0f);
@@ -49,7 +52,7 @@ struct EpiFwd {
     float *Z;
     __nv_bfloat16 *H;
     int N, act;
-    __device__ __forceinline__ void operator()(int row, int col, const float (&v)[8]) const {
+    __device__ __forceinline__ void operator()(int, int row, int col, const float (&v)[8]) const {
         const size_t o = static_cast<size_t>(row) * N + col;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -66,7 +69,7 @@ struct EpiBwd {
     const float *Zprev;
     __nv_bfloat16 *dX;
     int N;
-    __device__ __forceinline__ void operator()(int row, int col, const float (&v)[8]) const {
+    __device__ __forceinline__ void operator()(int, int row, int col, const float (&v)[8]) const {
         const size_t o = static_cast<size_t>(row) * N + col;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -92,9 +95,14 @@ __global__ void transpose_bf16_kernel(const __nv_bfloat16 *__restrict__ X, __nv_
 __global__ void colsum_kernel(const __nv_bfloat16 *__restrict__ dZ, float *__restrict__ db, int M, int N) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
-    float s = 0.0f;
-    for (int m = blockIdx.y; m < M; m += gridDim.y) s += __bfloat162float(dZ[static_cast<size_t>(m) * N + n]);
-    atomicAdd(&db[n], s);
+    float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // four independent chains keep several loads in flight
+    int m = blockIdx.y;
+    for (; m + 3 * static_cast<int>(gridDim.y) < M; m += 4 * gridDim.y) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s[u] += __bfloat162float(dZ[static_cast<size_t>(m + u * gridDim.y) * N + n]);
+    }
+    for (; m < M; m += gridDim.y) s[0] += __bfloat162float(dZ[static_cast<size_t>(m) * N + n]);
+    atomicAdd(&db[n], (s[0] + s[1]) + (s[2] + s[3]));
 }
 
 // Mean-squared error over the first T of ld columns: loss += scale * sum (p - t)^2 and
@@ -136,6 +144,15 @@ __global__ void adam_kernel(float *__restrict__ w, const float *__restrict__ g, 
         const int r = static_cast<int>(i / cols), c = static_cast<int>(i % cols);
         wt[static_cast<size_t>(c) * rows + r] = b;
     }
+}
+
+// D = sum over the splits of a split-K product's partials (fixed order: deterministic)
+__global__ void sum_splits_kernel(const float *__restrict__ work, float *__restrict__ D, size_t n, int splits) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float acc = 0.0f;
+    for (int z = 0; z < splits; ++z) acc += work[z * n + i];
+    D[i] = acc;
 }
 
 __global__ void ema_kernel(const float *__restrict__ w, float *__restrict__ avg, size_t n, float beta) {
@@ -224,13 +241,18 @@ template <class Epi> void set_smem_attr() {
 
 // Common checks and the launch of one tensor-core GEMM (asynchronous).
 template <class Epi>
-int launch_gemm(const void *A, const void *B, int M, int N, int K, const Epi &epi, void *stream, tmc_status *st) {
+int launch_gemm(const void *A, const void *B, int M, int N, int K, const Epi &epi, void *stream, tmc_status *st,
+                int splits = 1) {
     if (!A || !B) {
         put(st, TMC_BAD_ARGUMENT, "NULL argument");
         return TMC_BAD_ARGUMENT;
     }
     if (M < 1 || N < 1 || K < 64 || K % 64 != 0) {
         put(st, TMC_BAD_CONFIG, "tensor-core GEMM needs M, N >= 1 and K a positive multiple of 64");
+        return TMC_BAD_CONFIG;
+    }
+    if (splits < 1 || (K / 64) % splits != 0) {
+        put(st, TMC_BAD_CONFIG, "split-K needs K / 64 to be a multiple of the number of splits");
         return TMC_BAD_CONFIG;
     }
     const int dev = current_device();
@@ -246,7 +268,7 @@ int launch_gemm(const void *A, const void *B, int M, int N, int K, const Epi &ep
         set_smem_attr<EpiBwd>();
         g_attr[dev] = true;
     }
-    const dim3 grid((N + kBN - 1) / kBN, (M + kGemmBM - 1) / kGemmBM);
+    const dim3 grid((N + kBN - 1) / kBN, (M + kGemmBM - 1) / kGemmBM, splits);
     gemm_tc_kernel<kBN, Epi><<<grid, kGemmThreads, kGemmSmemRequest, static_cast<cudaStream_t>(stream)>>>(
         static_cast<const __nv_bfloat16 *>(A), static_cast<const __nv_bfloat16 *>(B), M, N, K, epi, status);
     const cudaError_t e = cudaGetLastError();
@@ -292,7 +314,7 @@ int tmc_b200_gemm_bf16(const uint16_t *A, const uint16_t *B, const float *bias, 
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaMemsetAsync(status, 0, sizeof(int), s);
-    const int rc = launch_gemm(A, B, M, N, K, EpiF32{D, bias, N}, stream, st);
+    const int rc = launch_gemm(A, B, M, N, K, EpiF32{D, bias, N, 0}, stream, st);
     if (rc != TMC_OK) return rc;
     const cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
@@ -335,7 +357,22 @@ int tmc_b200_nn_matmul_f32(const uint16_t *A, const uint16_t *B, float *D, int32
         put(st, TMC_BAD_ARGUMENT, "NULL argument");
         return TMC_BAD_ARGUMENT;
     }
-    return launch_gemm(A, B, M, N, K, EpiF32{D, nullptr, N}, stream, st);
+    return launch_gemm(A, B, M, N, K, EpiF32{D, nullptr, N, 0}, stream, st);
+}
+
+int tmc_b200_nn_matmul_f32_splitk(const uint16_t *A, const uint16_t *B, float *D, float *work, int32_t M, int32_t N,
+                                  int32_t K, int32_t splits, void *stream, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!D || !work) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument");
+        return TMC_BAD_ARGUMENT;
+    }
+    const size_t mn = static_cast<size_t>(M) * N;
+    const int rc = launch_gemm(A, B, M, N, K, EpiF32{work, nullptr, N, mn}, stream, st, splits);
+    if (rc != TMC_OK) return rc;
+    sum_splits_kernel<<<static_cast<unsigned>((mn + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        work, D, mn, splits);
+    return launched(st);
 }
 
 int tmc_b200_nn_transpose(const uint16_t *X, uint16_t *Y, int32_t rows, int32_t cols, void *stream,
@@ -359,7 +396,7 @@ int tmc_b200_nn_colsum(const uint16_t *dZ, float *db, int32_t M, int32_t N, void
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaMemsetAsync(db, 0, sizeof(float) * N, s);
-    colsum_kernel<<<dim3((N + 127) / 128, 64), 128, 0, s>>>(reinterpret_cast<const __nv_bfloat16 *>(dZ), db, M, N);
+    colsum_kernel<<<dim3((N + 127) / 128, 128), 128, 0, s>>>(reinterpret_cast<const __nv_bfloat16 *>(dZ), db, M, N);
     return launched(st);
 }
 

@@ -156,6 +156,11 @@ class Member:
         self.dZT = [torch.empty(n, batch, **bf) for (_, n) in LAYER_DIMS]
         self.XT = torch.empty(K_IN, batch, **bf)
         self.loss = torch.zeros(1, **f32)
+        # weight gradients contract over the batch: split it so that enough CTAs share the work
+        self.splits = max(1, min(8, batch // 512))
+        while (batch // 64) % self.splits:
+            self.splits -= 1
+        self.work = torch.empty(self.splits * max(n * k for (k, n) in LAYER_DIMS), **f32)
         self.step_count = 0
         self.L = L
 
@@ -184,7 +189,8 @@ class Member:
             k, n = LAYER_DIMS[li]
             _call("tmc_b200_nn_transpose", _p(self.dZ[li]), _p(self.dZT[li]), B, n, s)
             prev_T = self.XT if li == 0 else self.HT[li - 1]
-            _call("tmc_b200_nn_matmul_f32", _p(self.dZT[li]), _p(prev_T), _p(self.gW[li]), n, k, B, s)
+            _call("tmc_b200_nn_matmul_f32_splitk", _p(self.dZT[li]), _p(prev_T), _p(self.gW[li]), _p(self.work),
+                  n, k, B, self.splits, s)
             _call("tmc_b200_nn_colsum", _p(self.dZ[li]), _p(self.gb[li]), B, n, s)
             if li > 0:
                 _call("tmc_b200_nn_backward_data", _p(self.dZ[li]), _p(self.WT[li]), _p(self.Z[li - 1]),
