@@ -32,6 +32,23 @@ __device__ __forceinline__ float gelu_grad(float x) {
     return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
 }
 
+// Eight consecutive columns of a row start on a 16-byte boundary when the row length is a multiple
+// of 8 (bf16) / 4 (float32); then the epilogues move them with vector loads and stores (one
+// instruction per 8 bf16 or 4 floats instead of one per element).
+__device__ __forceinline__ uint4 pack8_bf16(const float (&x)[8]) {
+    uint4 u;
+    __nv_bfloat162 h;
+    h = __floats2bfloat162_rn(x[0], x[1]);
+    u.x = *reinterpret_cast<const uint32_t *>(&h);
+    h = __floats2bfloat162_rn(x[2], x[3]);
+    u.y = *reinterpret_cast<const uint32_t *>(&h);
+    h = __floats2bfloat162_rn(x[4], x[5]);
+    u.z = *reinterpret_cast<const uint32_t *>(&h);
+    h = __floats2bfloat162_rn(x[6], x[7]);
+    u.w = *reinterpret_cast<const uint32_t *>(&h);
+    return u;
+}
+
 // D (float32) = acc (+ bias); split z of a split-K product writes its partial at D + z * split_stride
 struct EpiF32 {
     float *D;
@@ -40,9 +57,17 @@ struct EpiF32 {
     size_t split_stride;
     __device__ __forceinline__ void operator()(int split, int row, int col, const float (&v)[8]) const {
         float *d = D + split * split_stride + static_cast<size_t>(row) * N + col;
+        float x[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
-            if (col + i < N) d[i] = v[i] + (bias ? bias[col + i] : 0.0f);
+        for (int i = 0; i < 8; ++i) x[i] = v[i] + ((bias && col + i < N) ? bias[col + i] : 0.0f);
+        if (N % 4 == 0 && col + 8 <= N) {
+            reinterpret_cast<float4 *>(d)[0] = make_float4(x[0], x[1], x[2], x[3]);
+            reinterpret_cast<float4 *>(d)[1] = make_float4(x[4], x[5], x[6], x[7]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (col + i < N) d[i] = x[i];
+        }
     }
 };
 
@@ -54,12 +79,25 @@ struct EpiFwd {
     int N, act;
     __device__ __forceinline__ void operator()(int, int row, int col, const float (&v)[8]) const {
         const size_t o = static_cast<size_t>(row) * N + col;
+        float z[8], h[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            if (col + i >= N) break;
-            const float z = v[i] + bias[col + i];
-            if (Z) Z[o + i] = z;
-            if (H) H[o + i] = __float2bfloat16_rn(act ? gelu(z) : z);
+            z[i] = v[i] + (col + i < N ? bias[col + i] : 0.0f);
+            h[i] = act ? gelu(z[i]) : z[i];
+        }
+        if (N % 8 == 0 && col + 8 <= N) {
+            if (Z) {
+                reinterpret_cast<float4 *>(Z + o)[0] = make_float4(z[0], z[1], z[2], z[3]);
+                reinterpret_cast<float4 *>(Z + o)[1] = make_float4(z[4], z[5], z[6], z[7]);
+            }
+            if (H) *reinterpret_cast<uint4 *>(H + o) = pack8_bf16(h);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (col + i >= N) break;
+                if (Z) Z[o + i] = z[i];
+                if (H) H[o + i] = __float2bfloat16_rn(h[i]);
+            }
         }
     }
 };
@@ -71,10 +109,20 @@ struct EpiBwd {
     int N;
     __device__ __forceinline__ void operator()(int, int row, int col, const float (&v)[8]) const {
         const size_t o = static_cast<size_t>(row) * N + col;
+        if (N % 8 == 0 && col + 8 <= N) {
+            const float4 z0 = reinterpret_cast<const float4 *>(Zprev + o)[0];
+            const float4 z1 = reinterpret_cast<const float4 *>(Zprev + o)[1];
+            const float z[8] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
+            float d[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            if (col + i >= N) break;
-            dX[o + i] = __float2bfloat16_rn(v[i] * gelu_grad(Zprev[o + i]));
+            for (int i = 0; i < 8; ++i) d[i] = v[i] * gelu_grad(z[i]);
+            *reinterpret_cast<uint4 *>(dX + o) = pack8_bf16(d);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (col + i >= N) break;
+                dX[o + i] = __float2bfloat16_rn(v[i] * gelu_grad(Zprev[o + i]));
+            }
         }
     }
 };
