@@ -27,10 +27,8 @@ constexpr int kBN = 128;
 constexpr int kGemmSmemRequest = 68 * 1024;
 static_assert(GemmSmem<128>::bytes <= kGemmSmemRequest, "GEMM shared memory");
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
-__device__ __forceinline__ float gelu_grad(float x) {
-    return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
-}
+__device__ __forceinline__ float gelu(float x) { return gelu_tanh(x); }
+__device__ __forceinline__ float gelu_grad(float x) { return gelu_tanh_grad(x); }
 
 // Eight consecutive columns of a row start on a 16-byte boundary when the row length is a multiple
 // of 8 (bf16) / 4 (float32); then the epilogues move them with vector loads and stores (one

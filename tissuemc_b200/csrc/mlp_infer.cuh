@@ -117,7 +117,7 @@ __global__ void pack_kernel(const __grid_constant__ PackParams P, unsigned char 
 }
 
 // ------------------------------------------------------------------------------ the fused kernel
-__device__ __forceinline__ float infer_gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float infer_gelu(float x) { return gelu_tanh(x); }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -282,6 +282,9 @@ __global__ void __launch_bounds__(kInferThreads, 1) ensemble_infer_kernel(const 
             epi_release(act_ready);
         }
         for (; ok && t < tiles; t += gridDim.x) {
+            float acc[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) acc[i] = 0.0f;
             float s1 = 0.0f, s2 = 0.0f;  // members' R_d on the grid: sum and sum of squares
             for (int m = 0; ok && m < P.members; ++m) {
                 const float *bias = P.bias + static_cast<size_t>(m) * kInferBiasPerMember;
@@ -293,41 +296,30 @@ __global__ void __launch_bounds__(kInferThreads, 1) ensemble_infer_kernel(const 
                     }
                     tc_fence_after();
                     if (l < 4) {
-                        // hidden layer: columns [128 j, 128 j + 128) of 512, 16 at a time, the TMEM
-                        // load of the next 16 in flight while these are processed; the bias as
-                        // 16-byte vector loads (one address across the warp)
+                        // hidden layer: columns [128 j, 128 j + 128) of 512, 16 at a time; the bias
+                        // as 16-byte vector loads (one address across the warp)
                         const float4 *b4 = reinterpret_cast<const float4 *>(bias + l * kInferHidden);
-                        uint32_t ra[16], rb[16];
-                        tmem_ld16_issue(lane_addr + static_cast<uint32_t>(j * 128), ra);
-                        tmem_ld16_wait(ra);
+#pragma unroll 1
+                        for (int c0 = j * 128; c0 < j * 128 + 128; c0 += 16) {
+                            float4 bb[4];
 #pragma unroll
-                        for (int step = 0; step < 8; ++step) {
-                            const int c0 = j * 128 + step * 16;
-                            uint32_t(&cur)[16] = (step & 1) ? rb : ra;
-                            uint32_t(&nxt)[16] = (step & 1) ? ra : rb;
-                            if (step < 7) tmem_ld16_issue(lane_addr + static_cast<uint32_t>(c0 + 16), nxt);
+                            for (int i = 0; i < 4; ++i) bb[i] = __ldg(b4 + (c0 >> 2) + i);
+                            float v[16];
+                            tmem_ld16(lane_addr + static_cast<uint32_t>(c0), v);
                             uint32_t w[8];
 #pragma unroll
                             for (int i = 0; i < 4; ++i) {
-                                const float4 bb = __ldg(b4 + (c0 >> 2) + i);
-                                w[2 * i] = pack_bf16x2(infer_gelu(__uint_as_float(cur[4 * i]) + bb.x),
-                                                       infer_gelu(__uint_as_float(cur[4 * i + 1]) + bb.y));
-                                w[2 * i + 1] = pack_bf16x2(infer_gelu(__uint_as_float(cur[4 * i + 2]) + bb.z),
-                                                           infer_gelu(__uint_as_float(cur[4 * i + 3]) + bb.w));
+                                w[2 * i] = pack_bf16x2(infer_gelu(v[4 * i] + bb[i].x), infer_gelu(v[4 * i + 1] + bb[i].y));
+                                w[2 * i + 1] =
+                                    pack_bf16x2(infer_gelu(v[4 * i + 2] + bb[i].z), infer_gelu(v[4 * i + 3] + bb[i].w));
                             }
                             *reinterpret_cast<uint4 *>(act_unit(A, r, c0)) = make_uint4(w[0], w[1], w[2], w[3]);
                             *reinterpret_cast<uint4 *>(act_unit(A, r, c0 + 8)) = make_uint4(w[4], w[5], w[6], w[7]);
-                            if (step < 7) tmem_ld16_wait(nxt);
                         }
                         epi_release(act_ready);
                     } else {
                         // output layer: columns [32 j, 32 j + 32) of 128
-                        // the ensemble mean accumulates in the output row itself (each thread owns
-                        // its row's 32 columns: no other thread touches them)
                         const float *b = bias + 4 * kInferHidden;
-                        const int g = t * 128 + r;
-                        float *orow = (P.out && g < P.n) ? P.out + static_cast<size_t>(g) * P.n_out : nullptr;
-                        const float inv_m = 1.0f / static_cast<float>(P.members);
                         float rd = 0.0f;
 #pragma unroll
                         for (int h = 0; h < 2; ++h) {
@@ -338,7 +330,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) ensemble_infer_kernel(const 
                                 const int c = j * 32 + h * 16 + i;
                                 if (c < P.n_out) {
                                     const float y = (v[i] + __ldg(b + c)) * __ldg(P.y_std + c) + __ldg(P.y_mean + c);
-                                    if (orow) orow[c] = (m == 0 ? 0.0f : orow[c]) + y * inv_m;
+                                    acc[h * 16 + i] += y;
                                     if (c < P.nbins) rd += exp10f(y) * __ldg(P.areas + c);
                                 }
                             }
@@ -363,7 +355,16 @@ __global__ void __launch_bounds__(kInferThreads, 1) ensemble_infer_kernel(const 
                         const bool last_member = m == P.members - 1;
                         const int next_t = last_member ? t + static_cast<int>(gridDim.x) : t;
                         if (last_member) {
+                            const int g = t * 128 + r;
                             if (g < P.n) {
+                                const float inv = 1.0f / static_cast<float>(P.members);
+                                if (P.out) {
+#pragma unroll
+                                    for (int i = 0; i < 32; ++i) {
+                                        const int c = j * 32 + i;
+                                        if (c < P.n_out) P.out[static_cast<size_t>(g) * P.n_out + c] = acc[i] * inv;
+                                    }
+                                }
                                 if (j == 0) {
                                     const float M = static_cast<float>(P.members);
                                     const float mean = s1 / M;

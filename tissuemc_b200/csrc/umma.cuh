@@ -19,6 +19,26 @@
 
 namespace tmc {
 
+// GELU in its tanh form, 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), with the SFU's tanh
+// (tanh.approx.f32), and its derivative. Used by training, by serving and by the CPU restatement of
+// the network alike, so the network is trained and served with the same activation.
+__device__ __forceinline__ float tanh_sfu(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float gelu_tanh(float x) {
+    const float u = 0.7978845608028654f * x * fmaf(0.044715f, x * x, 1.0f);
+    const float hx = 0.5f * x;
+    return fmaf(hx, tanh_sfu(u), hx);
+}
+__device__ __forceinline__ float gelu_tanh_grad(float x) {
+    const float x2 = x * x;
+    const float t = tanh_sfu(0.7978845608028654f * x * fmaf(0.044715f, x2, 1.0f));
+    const float du = 0.7978845608028654f * fmaf(3.0f * 0.044715f, x2, 1.0f);
+    return fmaf(0.5f * x * du, fmaf(-t, t, 1.0f), 0.5f * (1.0f + t));
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }

@@ -7,6 +7,9 @@ the network — forward, backward, loss, Adam — runs in this package's CUDA ke
 (``tmc_b200_nn_*``: tcgen05 tensor-core GEMMs with BF16 operands and FP32 accumulation, fused
 bias/GELU epilogues); torch only provides device buffers, random permutations and gathers.
 
+Activation: GELU in its tanh form, 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), evaluated with
+the SFU's tanh in training and serving alike.
+
 Encoding (13 inputs, 66 outputs):
   inputs   for layer slots 0..2: log10 mu_a, log10 mu_s', g, log10 thickness (an absent layer:
            zeros, and log10 thickness ABSENT_LOG_D), then the shared refractive index n;
