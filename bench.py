@@ -42,7 +42,9 @@ WORKLOADS = {
     "sweep": SWEEP_DESC,
     "surrogate": "learned surrogate trained on sweep solves; gated serving and inverse fits",
     "serve": "fused ensemble inference: 4 members of 13(64) -> 4x512 GELU -> 66(128), gate on the R_d spread",
+    "train": "surrogate training: 4 members, batch 4096 each, Adam + Polyak averaging, synthetic targets",
 }
+TRAIN_FLOP_PER_SAMPLE = 3 * 2 * (64 * 512 + 3 * 512 * 512 + 512 * 128)  # forward + two backward products
 SERVE_FLOP_PER_QUERY = 4 * 2 * (64 * 512 + 3 * 512 * 512 + 512 * 128)  # 7.08 MFLOP (padded shapes)
 METRIC = "photons/s on 1 B200 (plain MC)"
 
@@ -340,6 +342,48 @@ def run_serve(a) -> None:
         }), flush=True)
 
 
+def run_train(a) -> None:
+    """Surrogate training throughput: --steps optimiser steps of the 4-member ensemble (forward,
+    backward, Adam, averaging: every product on the tcgen05 kernels) on 65,536 synthetic samples;
+    value = samples per second over all members, timed with CUDA events."""
+    import numpy as np
+    import torch
+
+    from tissuemc_b200 import surrogate as S
+
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(rank)
+    X, Y = rng.normal(size=(65536, S.N_FEAT)), rng.normal(size=(65536, S.N_OUT))
+    ens = S.Ensemble(members=4, batch=4096, seed=0, device=f"cuda:{local}")
+    ens.train(X[:4096 * max(1, a.warmup)], Y[:4096 * max(1, a.warmup)], epochs=1, lr=1e-3, ema=0.999)
+    steps = max(1, a.steps)
+    n = 4096 * steps
+    Xs, Ys = np.resize(X, (n, S.N_FEAT)), np.resize(Y, (n, S.N_OUT))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        e0.record()
+        ens.train(Xs, Ys, epochs=1, lr=1e-3, ema=0.999)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    if rank == 0:
+        peak = float(_peaks().get("bf16_tflops", 1590.0))
+        achieved = 4 * 4096 * TRAIN_FLOP_PER_SAMPLE / (ms * 1e-3) / 1e12
+        print(json.dumps({
+            "metric": "surrogate training samples/s on 1 B200 (4-member ensemble)",
+            "value": 4 * 4096 / (ms * 1e-3), "unit": "samples/s", "n_gpus": world, "steps": steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 operands, fp32 accumulation and master weights", "data": "synthetic (random samples)",
+            "config": {"workload": f"train: {WORKLOADS['train']}"},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": "bf16_tflops (burst) of MEASURED_PEAKS.json; 3 x forward FLOPs per sample"},
+            "clocks": clk.summary(),
+        }), flush=True)
+
+
 def main() -> None:
     a = _args()
     if a.impl == "reference":
@@ -353,6 +397,9 @@ def main() -> None:
         return
     if a.workload == "serve":
         run_serve(a)
+        return
+    if a.workload == "train":
+        run_train(a)
         return
     import ctypes
 
