@@ -6,6 +6,12 @@
 
 namespace tmc {
 
+// 1: route a deposit with selects and one generic-address atomic; 0: branch to the shared or
+// global atomic (measured faster, the default)
+#ifndef TMC_DEPOSIT_GENERIC
+#define TMC_DEPOSIT_GENERIC 0
+#endif
+
 // Shared-memory layout of one block, in 64-bit words (offsets computed identically on the host).
 struct SmemLayout {
     int ring, batch, core_a, lastz_a, lastr_a, rd, tt, layers, total;  // word offsets / total words
@@ -65,6 +71,15 @@ template <int FAST> struct PlainCtx {
 
     // Deposit into A(r,z) at bin (ir, iz): the shared core tile, the shared cross, or global.
     __device__ __forceinline__ void deposit(int ir, int iz, unsigned long long v) const {
+#if TMC_DEPOSIT_GENERIC
+        // one generic-address atomic on the selected word (no divergent paths)
+        unsigned long long *p = &P.g_arz[static_cast<size_t>(ir) * P.nz + iz];
+        if (cross && ir == P.nr - 1) p = &s_lastr[iz];
+        if (cross && iz == P.nz - 1) p = &s_lastz[ir];
+        if (ir < P.tr_a && iz < P.tz_a) p = &s_core[ir * P.tz_a + iz];
+        atomicAdd(p, v);
+        return;
+#endif
         if (ir < P.tr_a && iz < P.tz_a) {
             atomicAdd(&s_core[ir * P.tz_a + iz], v);
         } else if (cross && iz == P.nz - 1) {
