@@ -1,0 +1,46 @@
+"""bench.py on the CPU: the reference arm's JSON line (it times the reference's own CPU engine)
+and the clock-sample parser that flags throttled runs."""
+
+from __future__ import annotations
+
+import json
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+import oracle
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="oracle/_ref/tissuemc not built")
+def test_reference_arm_prints_one_json_line():
+    p = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--workload", "slab_n14",
+                        "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert p.returncode == 0, p.stderr
+    lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "photons/s" and d["value"] > 0
+    assert d["higher_is_better"] is True and d["steps"] == 1
+    assert d["e2e"] == {"value": d["value"], "unit": "photons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and "slab_n14" in cb["sample"]
+
+
+def test_clock_summary_reads_throttle_reasons():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    c = bench.Clocks(0)
+    c.lines = ["0, 1965, 1965, 700.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+               "0, 1320, 1965, 998.7, 0x4, Not Active, Not Active, Not Active, Active",
+               "0, 1800, 1965, 900.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+               "garbage line"]
+    s = c.summary()
+    assert s["samples"] == 3 and s["sm_mhz"] == 1800.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"]
+    c.lines = ["0, 900, 1965, 400.0, 0x8, Active, Not Active, Active, Not Active"]
+    assert c.summary()["reasons"] == ["hw_slowdown", "sw_thermal_slowdown"]
