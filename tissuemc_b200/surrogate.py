@@ -263,6 +263,8 @@ class Ensemble:
         xb = t.empty(self.B, K_IN, dtype=t.bfloat16, device=self.dev)
         yb = t.empty(self.B, N_OUT, dtype=t.float32, device=self.dev)
         k = 0
+        t_start, t_end = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
+        t_start.record()
         avg = []
         if ema > 0:
             avg = [([w.clone() for w in m.W], [b.clone() for b in m.b]) for m in self.members]
@@ -286,6 +288,9 @@ class Ensemble:
                                   ctypes.c_void_p(stream))
                 k += 1
             self.history.append(float(acc.item()) / (steps * len(self.members)))
+        t_end.record()
+        t_end.synchronize()
+        self.last_step_ms = t_start.elapsed_time(t_end) / max(1, total)  # device time per optimiser step
         for m, (aw, ab) in zip(self.members, avg):
             for li, (w, b) in enumerate(zip(aw, ab, strict=True)):
                 m.W[li].copy_(w)
