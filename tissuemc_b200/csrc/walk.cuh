@@ -116,8 +116,12 @@ __device__ __forceinline__ void philox4x32_10_rk(uint32_t c0, uint32_t c1, uint3
 }
 
 // Uniform on (0,1) from one word, keeping 23 bits (philox.hpp:133-136).
+// The value is ((x >> 9) + 1/2) * 2^-23, computed without an integer-to-float conversion: the 23
+// kept bits become the mantissa of a float in [1, 2), 1 + m 2^-23, and subtracting 1 - 2^-24 gives
+// (2m + 1) 2^-24 exactly (an odd integer below 2^24 times a power of two), bit for bit the
+// reference's value.
 __device__ __forceinline__ float unit_open(uint32_t x) {
-    return (static_cast<float>(x >> 9) + 0.5f) * 0x1p-23f;
+    return __fsub_rn(__uint_as_float((x >> 9) | 0x3F800000u), 0x1.fffffep-1f);
 }
 
 // ------------------------------------------------------------------------------------ math
