@@ -47,6 +47,11 @@ WORKLOADS = {
 TRAIN_FLOP_PER_SAMPLE = 3 * 2 * (64 * 512 + 3 * 512 * 512 + 512 * 128)  # forward + two backward products
 SERVE_FLOP_PER_QUERY = 4 * 2 * (64 * 512 + 3 * 512 * 512 + 512 * 128)  # 7.08 MFLOP (padded shapes)
 METRIC = "photons/s on 1 B200 (plain MC)"
+# DRAM bytes (read + write) of one walk launch, from one ncu capture of the full skin5 launch
+# (1e8 photons; dram__bytes_read.sum 2.41 / 2.71 MB over two launches, dram__bytes_write.sum 0):
+# the tally buffer's compulsory reads; the tallies stay in shared memory and L2, so the traffic
+# does not grow with the photons.
+WALK_DRAM_BYTES = {"skin5": 2.56e6}
 
 # Algorithmic work of the walk, counted from the reference's step (include/tissuemc/physics.hpp
 # :148-193 and :101-144 with the scoring) and frozen here: FP32 operations and SFU operations
@@ -524,7 +529,8 @@ def main() -> None:
             "gpu_launches": a.steps,
             "roofline": {
                 "bound": "sfu" if s_tot / 16.0 >= f_tot / 128.0 else "fp32", "achieved": achieved / 1e9,
-                "peak": peak / 1e9, "unit": "Gphotons/s", "frac": achieved / peak, "traffic": None,
+                "peak": peak / 1e9, "unit": "Gphotons/s", "frac": achieved / peak,
+                "traffic": WALK_DRAM_BYTES.get(a.workload) if not a.photons else None,
                 "peak_source": f"issue roofline: {n_sm} SMs x {f_mhz:.0f} MHz (sm_max_mhz of MEASURED_PEAKS.json) / "
                                f"max(F/128, S/16) with F={f_tot:.0f} FP32 and S={s_tot:.0f} SFU ops per photon",
             },
