@@ -223,6 +223,13 @@ def _check_fused_against_layered(S, ens, X):
     assert np.abs(sp - ref_sp).max() <= 2e-3 + 0.05 * ref_sp.max()
     near = np.abs(ref_sp - fs.threshold) < 2e-3
     assert np.array_equal(route[~near], (ref_sp > fs.threshold)[~near])
+    # the per-layer serving path (encode kernel, member GEMMs, gate kernel) agrees as well
+    sp_l: list = []
+    y_l, rd_l, route_l = S.Server(ens, chunk=65536)(X, sp_l)
+    assert np.abs(y_l - ref_y).max() <= 1e-2 * np.abs(ref_y).max()
+    np.testing.assert_allclose(rd_l, ref_rd, rtol=2e-2)
+    assert np.abs(sp_l[0] - ref_sp).max() <= 2e-3 + 0.05 * ref_sp.max()
+    assert np.array_equal(route_l[~near], (ref_sp > fs.threshold)[~near])
 
 
 def test_fused_ensemble_kernel_matches_the_layered_path_random_weights():

@@ -337,9 +337,11 @@ def rd_total(y_raw: np.ndarray, dr: float = 0.01) -> np.ndarray:
 
 
 class Server:
-    """Gated serving on the device: encode, every member's forward pass and the gate run in this
-    package's kernels on one stream; the host sends raw features and receives the ensemble mean
-    outputs, the members' mean R_d on the grid and the routing flags."""
+    """Gated serving layer by layer (the path before the fused kernel, kept as its cross-check):
+    encode, every member's forward pass through the per-layer tensor-core GEMMs, and the gate
+    kernel, on one stream; the host sends raw features and receives the ensemble mean outputs, the
+    members' mean R_d on the grid and the routing flags. `FusedServer` does the same in one launch
+    and is what serving uses."""
 
     def __init__(self, ens: Ensemble, chunk: int = 65536, threshold: float = 0.01):
         import torch
