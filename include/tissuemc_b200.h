@@ -364,6 +364,16 @@ TMC_B200_API int tmc_b200_nn_ensemble_infer(const uint8_t *packed, const float *
                                             float *out, float *rd_mean, float *spread, uint8_t *route, void *stream,
                                             tmc_status *status);
 
+/* Physics probe: the walk's own device functions in isolation, on many Philox streams keyed by
+ * (seed, thread), for unit tests of the GPU physics (TissueMC checks its CPU physics the same way,
+ * tests/cpp/test_physics.cpp:91-160). One layer with anisotropy g and attenuation mu_t [1/cm];
+ * fast_math as in tmc_options. out[5] (host): what 0 = Henyey-Greenstein cosines: sum, sum of
+ * squares, min, max; what 1 = consecutive direction rotations (32 chains): worst |norm - 1|;
+ * what 2 = free paths: sum, sum of squares. out[4] = the samples drawn (samples rounded up to a
+ * multiple of the threads). No reference counterpart; allocates a 32-byte device buffer. */
+TMC_B200_API int tmc_b200_probe_physics(int32_t what, double g, double mu_t, int64_t samples, uint64_t seed,
+                                        int32_t fast_math, int32_t device, double *out, tmc_status *status);
+
 /* Parse an MCML .mci file (the reference's parse_mci_file, src/io/mci.cpp:173-183): writes up to
  * `max_runs` runs and returns the number found in *n_runs. Errors carry the line number. */
 TMC_B200_API int tmc_b200_parse_mci(const char *path, tmc_run_spec *runs, int32_t max_runs, int32_t *n_runs,

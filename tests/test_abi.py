@@ -217,3 +217,9 @@ def test_run_without_a_device_fails_loudly():
         tmc.run(_spec(), batches=2)
     assert e.value.code == tmc.NO_DEVICE and "no usable CUDA device found" in str(e.value)
     assert not tmc.available()
+
+
+def test_physics_probe_rejects_bad_arguments_before_touching_a_device():
+    for kw in ({"what": "hg", "g": 1.0}, {"what": "step", "g": 0.5, "mu_t": 0.0}, {"what": "hg", "g": 0.5, "samples": 0}):
+        with pytest.raises(tmc.ConfigError, match="probe"):
+            tmc.probe_physics(**kw)

@@ -302,3 +302,35 @@ def test_slab_identical_photons_vs_the_reference_cuda_engine(slab, slab_gpu, tmp
     assert p.returncode == 0, p.stderr
     ref = from_reference_json(json.loads(out.read_text())["runs"][0])
     _assert_gaps(identical_photon_gaps(ref, from_engine(slab_gpu), profiles=("a_z", "rd_r")))
+
+
+# ---- the walk's device physics in isolation (tmc_b200_probe_physics), checked the way the
+# reference checks its CPU physics (tests/cpp/test_physics.cpp:91-160)
+
+@pytest.mark.parametrize("fast", [True, False])
+@pytest.mark.parametrize("g", [0.0, 0.5, 0.9, -0.3])
+def test_device_hg_sampler_reproduces_its_first_two_moments(g, fast):
+    r = tmc.probe_physics("hg", g, samples=1_000_000, seed=7, fast_math=fast)
+    assert r["samples"] >= 1_000_000
+    assert -1.0 <= r["min"] and r["max"] <= 1.0
+    # E[cos] = g and E[cos^2] = (1 + 2 g^2) / 3; the standard error is below 5.8e-4: ~5 sigma
+    assert abs(r["mean"] - g) < 3e-3
+    assert abs(r["mean_square"] - (1 + 2 * g * g) / 3) < 3e-3
+
+
+@pytest.mark.parametrize("fast", [True, False])
+@pytest.mark.parametrize("g", [0.0, 0.99])
+def test_device_direction_stays_unit_over_millions_of_scatterings(g, fast):
+    """32 directions each turned 4e6 times in a row (g = 0.99 keeps consecutive directions close,
+    where an unnormalised rotation would drift); the reference's float32 limit is 5e-7."""
+    r = tmc.probe_physics("rotate", g, samples=32 * 4_000_000, seed=11, fast_math=fast)
+    assert r["worst_norm_error"] < 5e-7
+
+
+@pytest.mark.parametrize("fast", [True, False])
+def test_device_free_paths_are_exponential_with_mean_one_over_mu_t(fast):
+    mu_t = 10.0
+    r = tmc.probe_physics("step", 0.75, mu_t=mu_t, samples=2_000_000, seed=3, fast_math=fast)
+    se = (1 / mu_t) / math.sqrt(r["samples"])
+    assert abs(r["mean"] - 1 / mu_t) < 5 * se
+    assert abs(r["mean_square"] - 2 / mu_t ** 2) < 5 * math.sqrt(20) * se / mu_t

@@ -145,6 +145,9 @@ PROTOTYPES = {
     "tmc_b200_run_static": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _P(CResult), _P(CStatus)]),
     "tmc_b200_run_device_range": (ctypes.c_int, [_P(CRunSpec), _P(COptions), ctypes.c_uint64, ctypes.c_uint64,
                                                   ctypes.c_void_p, ctypes.c_void_p, _P(CStatus)]),
+    "tmc_b200_probe_physics": (ctypes.c_int, [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int64,
+                                              ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32,
+                                              _P(ctypes.c_double), _P(CStatus)]),
     "tmc_b200_write_mco": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _P(CResult), ctypes.c_char_p, _P(CStatus)]),
     "tmc_b200_sweep_default_options": (None, [_P(CSweepOptions)]),
     "tmc_b200_sweep_sample": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int32, _P(CSweepConfig), _P(CStatus)]),
@@ -453,6 +456,25 @@ def run_device_range(spec: RunSpec, opt: COptions, first_photon: int, count: int
     _check(lib().tmc_b200_run_device_range(ctypes.byref(c), ctypes.byref(opt), first_photon, count,
                                            ctypes.c_void_p(d_tally_ptr), ctypes.c_void_p(stream_ptr),
                                            ctypes.byref(st)), st)
+
+
+def probe_physics(what: str, g: float, mu_t: float = 10.0, samples: int = 1_000_000, seed: int = 7,
+                  fast_math: bool = True, device: int = 0) -> dict:
+    """Run the walk's device physics in isolation (tmc_b200_probe_physics): what = "hg"
+    (Henyey-Greenstein cosines), "rotate" (consecutive rotations of one direction) or "step"
+    (free paths). Returns the sums, extremes and sample count."""
+    out = (ctypes.c_double * 5)()
+    st = CStatus()
+    code = {"hg": 0, "rotate": 1, "step": 2}[what]
+    _check(lib().tmc_b200_probe_physics(code, g, mu_t, samples, seed, int(fast_math), device, out,
+                                        ctypes.byref(st)), st)
+    n = out[4]
+    if code == 1:
+        return {"worst_norm_error": out[0], "samples": n}
+    r = {"mean": out[0] / n, "mean_square": out[1] / n, "samples": n}
+    if code == 0:
+        r["min"], r["max"] = out[2], out[3]
+    return r
 
 
 def shard_range(photons: int, rank: int, world: int) -> tuple[int, int]:

@@ -29,7 +29,7 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 CXX_FLAGS = ["-std=c++17", "-O3", "-fPIC", "-Wall", "-Wextra", "-fvisibility=hidden"]
 
 # The shared library: kernels, C ABI and the C++ it needs (exports only the C ABI).
-CUDA_SOURCES = ["engine.cu", "sweep.cu", "mlp.cu"]
+CUDA_SOURCES = ["engine.cu", "sweep.cu", "mlp.cu", "probe.cu"]
 HOST_SOURCES = ["host/engine_host.cpp", "host/mci.cpp", "host/abi_mci.cpp", "host/mco.cpp"]
 # The CLI: the reference-shaped C++ host code, linked against the library's C ABI.
 CLI_SOURCES = ["host/cli.cpp", "host/run_cuda.cpp", "host/result.cpp", "host/mci.cpp"]

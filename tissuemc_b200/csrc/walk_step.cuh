@@ -85,6 +85,71 @@ template <int FAST> __device__ __forceinline__ int bin_of(float x, float width, 
     return static_cast<int>(fminf(fmaxf(i, 0.0f), static_cast<float>(n - 1)));
 }
 
+// Free path -ln(u) / mu_t of an interaction step (physics.hpp:148-158).
+template <int FAST> __device__ __forceinline__ float step_length(const Hot &h, float u) {
+    if constexpr (Math<FAST>::log) {
+        // the SFU logarithm's absolute error can flip the sign of log(u) for the two largest u of
+        // the 23-bit grid; a step is never negative
+        return fmul(fmaxf(-m_log<FAST>(u), 0.0f), h.inv_mut);
+    } else if constexpr (Math<FAST>::div) {
+        return fmul(-m_log<FAST>(u), h.inv_mut);
+    } else {
+        return -m_log<FAST>(u) / h.mut;
+    }
+}
+
+// Henyey-Greenstein cosine of the scattering angle from one uniform draw (physics.hpp:101-113).
+template <int FAST> __device__ __forceinline__ float hg_cos(const Hot &h, float xi) {
+    if (h.g == 0.0f) return ffma(2.0f, xi, -1.0f);
+    const float t = m_div<FAST>(h.hg_a, ffma(h.hg_c, xi, h.hg_b));
+    float ct;
+    if constexpr (Math<FAST>::div) ct = fmul(ffma(-t, t, h.hg_d), h.inv_2g);
+    else ct = ffma(-t, t, h.hg_d) / h.hg_c;
+    return fminf(fmaxf(ct, -1.0f), 1.0f);
+}
+
+// Turn the direction by the polar cosine ct and the azimuth 2 pi u, then renormalise it
+// (physics.hpp:116-144).
+template <int FAST>
+__device__ __forceinline__ void rotate(float &ux, float &uy, float &uz, float ct, float u) {
+    float st = ffma(-ct, ct, 1.0f);
+    st = st > 0.0f ? m_sqrt<FAST>(st) : 0.0f;
+    float sp, cp;
+    if constexpr (Math<FAST>::sincos) {
+        // psi - pi lies in (-pi, pi), where the SFU sine and cosine are accurate
+        __sincosf(fmul(kTwoPi, fsub(u, 0.5f)), &sp, &cp);
+        sp = -sp;
+        cp = -cp;
+    } else {
+        sincosf(fmul(kTwoPi, u), &sp, &cp);
+    }
+    if (fabsf(uz) > kCosZero) {
+        ux = fmul(st, cp);
+        uy = fmul(st, sp);
+        uz = uz >= 0.0f ? ct : -ct;
+    } else {
+        const float ox = ux, oy = uy, oz = uz;
+        const float q = ffma(-oz, oz, 1.0f);  // 1 - uz^2
+        const float ix = ffma(fmul(ox, oz), cp, -fmul(oy, sp));
+        const float iy = ffma(fmul(oy, oz), cp, fmul(ox, sp));
+        if constexpr (Math<FAST>::sqrt) {
+            const float it = rsqrtf(q);
+            ux = ffma(fmul(st, ix), it, fmul(ox, ct));
+            uy = ffma(fmul(st, iy), it, fmul(oy, ct));
+            uz = ffma(fmul(fmul(-st, cp), q), it, fmul(oz, ct));
+        } else {
+            const float tmp = sqrtf(q);
+            ux = fadd(fmul(st, ix) / tmp, fmul(ox, ct));
+            uy = fadd(fmul(st, iy) / tmp, fmul(oy, ct));
+            uz = ffma(fmul(-st, cp), tmp, fmul(oz, ct));
+        }
+    }
+    const float inv = m_rsqrt<FAST>(norm2(ux, uy, uz));
+    ux = fmul(ux, inv);
+    uy = fmul(uy, inv);
+    uz = fmul(uz, inv);
+}
+
 // Radial distance of the packet from the source axis (the r of A(r,z), R_d(r,a), T_t(r,a)).
 template <int FAST> __device__ __forceinline__ float radius(float x, float y) { return m_sqrt<FAST>(norm2(x, y)); }
 
@@ -123,16 +188,7 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
     ++L.steps;
     float s;
     if (L.sleft == 0.0f) {
-        const float u = unit_open(C.draw(L));
-        if constexpr (Math<FAST>::log) {
-            // the SFU logarithm's absolute error can flip the sign of log(u) for the two largest
-            // u of the 23-bit grid; a step is never negative
-            s = fmul(fmaxf(-m_log<FAST>(u), 0.0f), L.h.inv_mut);
-        } else if constexpr (Math<FAST>::div) {
-            s = fmul(-m_log<FAST>(u), L.h.inv_mut);
-        } else {
-            s = -m_log<FAST>(u) / L.h.mut;
-        }
+        s = step_length<FAST>(L.h, unit_open(C.draw(L)));
     } else {
         if constexpr (Math<FAST>::div) s = fmul(L.sleft, L.h.inv_mut);
         else s = L.sleft / L.h.mut;
@@ -197,57 +253,8 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
         L.run_abs += v;
         C.absorb(L, v);
         // ---- spin (physics.hpp:101-144)
-        float ct;
-        {
-            const float xi = unit_open(C.draw(L));
-            if (L.h.g == 0.0f) {
-                ct = ffma(2.0f, xi, -1.0f);
-            } else {
-                const float t = m_div<FAST>(L.h.hg_a, ffma(L.h.hg_c, xi, L.h.hg_b));
-                if constexpr (Math<FAST>::div) ct = fmul(ffma(-t, t, L.h.hg_d), L.h.inv_2g);
-                else ct = ffma(-t, t, L.h.hg_d) / L.h.hg_c;
-                ct = fminf(fmaxf(ct, -1.0f), 1.0f);
-            }
-        }
-        float st = ffma(-ct, ct, 1.0f);
-        st = st > 0.0f ? m_sqrt<FAST>(st) : 0.0f;
-        float sp, cp;
-        {
-            const float u = unit_open(C.draw(L));
-            if constexpr (Math<FAST>::sincos) {
-                // psi - pi lies in (-pi, pi), where the SFU sine and cosine are accurate
-                __sincosf(fmul(kTwoPi, fsub(u, 0.5f)), &sp, &cp);
-                sp = -sp;
-                cp = -cp;
-            } else {
-                sincosf(fmul(kTwoPi, u), &sp, &cp);
-            }
-        }
-        if (fabsf(L.uz) > kCosZero) {
-            L.ux = fmul(st, cp);
-            L.uy = fmul(st, sp);
-            L.uz = L.uz >= 0.0f ? ct : -ct;
-        } else {
-            const float ox = L.ux, oy = L.uy, oz = L.uz;
-            const float q = ffma(-oz, oz, 1.0f);  // 1 - uz^2
-            const float ix = ffma(fmul(ox, oz), cp, -fmul(oy, sp));
-            const float iy = ffma(fmul(oy, oz), cp, fmul(ox, sp));
-            if constexpr (Math<FAST>::sqrt) {
-                const float it = rsqrtf(q);
-                L.ux = ffma(fmul(st, ix), it, fmul(ox, ct));
-                L.uy = ffma(fmul(st, iy), it, fmul(oy, ct));
-                L.uz = ffma(fmul(fmul(-st, cp), q), it, fmul(oz, ct));
-            } else {
-                const float tmp = sqrtf(q);
-                L.ux = fadd(fmul(st, ix) / tmp, fmul(ox, ct));
-                L.uy = fadd(fmul(st, iy) / tmp, fmul(oy, ct));
-                L.uz = ffma(fmul(-st, cp), tmp, fmul(oz, ct));
-            }
-        }
-        const float inv = m_rsqrt<FAST>(norm2(L.ux, L.uy, L.uz));
-        L.ux = fmul(L.ux, inv);
-        L.uy = fmul(L.uy, inv);
-        L.uz = fmul(L.uz, inv);
+        const float ct = hg_cos<FAST>(L.h, unit_open(C.draw(L)));
+        rotate<FAST>(L.ux, L.uy, L.uz, ct, unit_open(C.draw(L)));
     }
 
     if (exit_kind) {
