@@ -170,3 +170,41 @@ def test_single_configuration_and_sixteen_layers():
     res = tmc.sweep_run(cfgs, opt, raw=True)
     r = _single_run_raw(cfgs[0], opt)
     assert np.array_equal(res.raw[0], r.raw)
+
+
+@pytest.mark.gpu
+def test_full_size_sweep_properties():
+    """The 4096-configuration sweep at its full photon counts (9.1e8 photons): for every
+    configuration the 2-D tallies are exact integer refinements of the batch totals (sum of
+    A(r,z) = sum of absorbed, of R_d(r,a) = R_d, of T_t(r,a) = T_t), no anomaly, and energy is
+    conserved within its batch spread."""
+    opt = tmc.sweep_options()
+    cfgs = tmc.sweep_sample(1, 4096)
+    res = tmc.sweep_run(cfgs, opt, raw=True)
+    nb, nr, nz, na = opt.batches, opt.nr, opt.nz, opt.na
+    lmax = (res.raw.shape[1] - nr * nz - 2 * nr * na) // nb - 4
+    assert res.raw.shape[0] == 4096
+    worst = 0.0
+    for i, c in enumerate(cfgs):
+        block = res.raw[i]
+        rows = block[: nb * (4 + lmax)].reshape(nb, 4 + lmax)
+        a_rz = block[nb * (4 + lmax): nb * (4 + lmax) + nr * nz]
+        rd_ra = block[nb * (4 + lmax) + nr * nz: nb * (4 + lmax) + nr * nz + nr * na]
+        tt_ra = block[nb * (4 + lmax) + nr * nz + nr * na:]
+        with np.errstate(over="ignore"):
+            assert a_rz.sum(dtype=np.uint64) == rows[:, 4:].sum(dtype=np.uint64), i
+            assert rd_ra.sum(dtype=np.uint64) == rows[:, 0].sum(dtype=np.uint64), i
+            assert tt_ra.sum(dtype=np.uint64) == rows[:, 1].sum(dtype=np.uint64), i
+        assert not rows[:, 3].any(), i  # anomalies
+        assert rows[:, 2].all(), i  # events in every batch
+        spec = tmc.config_spec(c, opt)
+        rsp = ((spec.n_above - spec.layers[0][0]) / (spec.n_above + spec.layers[0][0])) ** 2
+        per = np.full(nb, int(c.photons) // nb, dtype=np.float64)
+        per[: int(c.photons) % nb] += 1
+        resid = (rows[:, 0] + rows[:, 1] + rows[:, 4:].sum(1)).astype(np.float64) / 2.0**32 / per + rsp - 1.0
+        se = resid.std(ddof=1) / math.sqrt(nb)
+        z = abs(resid.mean()) / (se + 1e-12)
+        # a family-wise bound over 4096 configurations (t with 9 degrees of freedom)
+        assert abs(resid.mean()) <= 8 * se + 1e-6, (i, resid.mean(), se)
+        worst = max(worst, z)
+    print(f"worst conservation |z| over 4096 configurations: {worst:.2f}")
