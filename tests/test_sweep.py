@@ -177,14 +177,15 @@ def test_full_size_sweep_properties():
     """The 4096-configuration sweep at its full photon counts (9.1e8 photons): for every
     configuration the 2-D tallies are exact integer refinements of the batch totals (sum of
     A(r,z) = sum of absorbed, of R_d(r,a) = R_d, of T_t(r,a) = T_t), no anomaly, and energy is
-    conserved within its batch spread."""
+    conserved within its batch spread and the float32 transport's rounding drift — the worst
+    configuration's residual equals the float32 CPU engine's on identical photons."""
     opt = tmc.sweep_options()
     cfgs = tmc.sweep_sample(1, 4096)
     res = tmc.sweep_run(cfgs, opt, raw=True)
     nb, nr, nz, na = opt.batches, opt.nr, opt.nz, opt.na
     lmax = (res.raw.shape[1] - nr * nz - 2 * nr * na) // nb - 4
     assert res.raw.shape[0] == 4096
-    worst = 0.0
+    worst, worst_i, worst_resid = -1.0, 0, None
     for i, c in enumerate(cfgs):
         block = res.raw[i]
         rows = block[: nb * (4 + lmax)].reshape(nb, 4 + lmax)
@@ -203,8 +204,20 @@ def test_full_size_sweep_properties():
         per[: int(c.photons) % nb] += 1
         resid = (rows[:, 0] + rows[:, 1] + rows[:, 4:].sum(1)).astype(np.float64) / 2.0**32 / per + rsp - 1.0
         se = resid.std(ddof=1) / math.sqrt(nb)
-        z = abs(resid.mean()) / (se + 1e-12)
-        # a family-wise bound over 4096 configurations (t with 9 degrees of freedom)
-        assert abs(resid.mean()) <= 8 * se + 1e-6, (i, resid.mean(), se)
-        worst = max(worst, z)
-    print(f"worst conservation |z| over 4096 configurations: {worst:.2f}")
+        # a family-wise bound over 4096 configurations (t with 9 degrees of freedom), plus the
+        # float32 weight's rounding drift, which grows with the interactions per photon
+        events = rows[:, 2].sum() / int(c.photons)
+        assert abs(resid.mean()) <= 8 * se + 1e-6 + 1e-8 * events, (i, resid.mean(), se, events)
+        if abs(resid.mean()) > worst:
+            worst, worst_i, worst_resid = abs(resid.mean()), i, resid
+    # the largest residual is the float32 transport's own: the CPU engine in float32 on identical
+    # photons leaves the same one
+    c = cfgs[worst_i]
+    spec = tmc.config_spec(c, opt)
+    o = oracle.run(oracle.Spec(layers=list(spec.layers), dz=spec.dz, dr=spec.dr, nz=spec.nz, nr=spec.nr, na=spec.na,
+                               n_above=spec.n_above, n_below=spec.n_below),
+                   int(c.photons), nb, int(c.seed), 32, threads=0)
+    o_resid = (o.rd + o.tt + o.absorbed.sum(1)) / o.photons + o.specular - 1.0
+    print(f"worst conservation residual {worst_resid.mean():.3e} (configuration {worst_i}); float32 CPU engine "
+          f"{o_resid.mean():.3e}")
+    assert abs(worst_resid.mean() - o_resid.mean()) <= 0.05 * abs(o_resid.mean()) + 1e-8
