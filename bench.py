@@ -489,7 +489,8 @@ def main() -> None:
         else:
             with torch.cuda.stream(stream):
                 walk()
-            host = d_tally.cpu()  # synchronises the stream
+            stream.synchronize()  # the walk and the all-reduce ran on `stream`, not the current one
+            host = d_tally.cpu()
             res = tmc.decode(spec, opt, host.numpy().view(np.uint64))
             res.device = torch.cuda.get_device_name(local)
         if i:  # the first call is a warm-up
