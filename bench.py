@@ -101,6 +101,28 @@ def _peaks() -> dict:
     return {}
 
 
+def _peak(key: str, fallback: float) -> tuple[float, str]:
+    """A roofline denominator: `key` of MEASURED_PEAKS.json (searched through nested objects) when
+    the file has it, else `fallback` (an earlier measurement on B200s of the same kind); returns the
+    value and a note saying which."""
+
+    def find(obj):
+        if isinstance(obj, dict):
+            v = obj.get(key)
+            if isinstance(v, (int, float)) and not isinstance(v, bool):
+                return float(v)
+            for sub in obj.values():
+                got = find(sub)
+                if got is not None:
+                    return got
+        return None
+
+    v = find(_peaks())
+    if v is not None:
+        return v, f"{key} of MEASURED_PEAKS.json (measured)"
+    return fallback, f"fallback {fallback:g} (MEASURED_PEAKS.json has no {key})"
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region (SM clock and throttle reasons)."""
 
@@ -326,8 +348,7 @@ def run_serve(a) -> None:
             e2e_t.append(time.perf_counter() - t0)
     e2e_s = sum(e2e_t) / len(e2e_t)
     if rank == 0:
-        peaks = _peaks()
-        peak = float(peaks.get("bf16_tflops", 1590.0))
+        peak, peak_note = _peak("bf16_tflops", 1590.0)
         achieved = n * SERVE_FLOP_PER_QUERY / (ms * 1e-3) / 1e12
         print(json.dumps({
             "metric": "surrogate queries/s on 1 B200 (fused ensemble kernel)", "value": n / (ms * 1e-3),
@@ -341,7 +362,7 @@ def run_serve(a) -> None:
             "gpu_launches": a.steps,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None,
-                         "peak_source": "bf16_tflops (burst) of MEASURED_PEAKS.json; algorithmic FLOPs of the "
+                         "peak_source": f"bf16 burst peak: {peak_note}; algorithmic FLOPs of the "
                                         "padded layers, 7.08 MFLOP per query"},
             "clocks": clk.summary(),
         }), flush=True)
@@ -350,7 +371,9 @@ def run_serve(a) -> None:
 def run_train(a) -> None:
     """Surrogate training throughput: --steps optimiser steps of the 4-member ensemble (forward,
     backward, Adam, averaging: every product on the tcgen05 kernels) on synthetic samples;
-    value = samples per second over all members, CUDA events around the steps."""
+    value = samples per second over all members, CUDA events around the steps that replay the
+    captured step graph (the first step of the call, launched from the host while the graph is
+    captured, is not timed)."""
     import numpy as np
     import torch
 
@@ -367,9 +390,9 @@ def run_train(a) -> None:
     Xs, Ys = np.resize(X, (n, S.N_FEAT)), np.resize(Y, (n, S.N_OUT))
     with Clocks(local) as clk:
         ens.train(Xs, Ys, epochs=1, lr=1e-3, ema=0.999)
-    ms = ens.last_step_ms  # CUDA events around the optimiser steps (data upload and setup excluded)
+    ms = ens.last_step_ms  # CUDA events around the replayed optimiser steps (data upload and setup excluded)
     if rank == 0:
-        peak = float(_peaks().get("bf16_tflops", 1590.0))
+        peak, peak_note = _peak("bf16_tflops", 1590.0)
         achieved = 4 * 4096 * TRAIN_FLOP_PER_SAMPLE / (ms * 1e-3) / 1e12
         print(json.dumps({
             "metric": "surrogate training samples/s on 1 B200 (4-member ensemble)",
@@ -379,7 +402,7 @@ def run_train(a) -> None:
             "config": {"workload": f"train: {WORKLOADS['train']}"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None,
-                         "peak_source": "bf16_tflops (burst) of MEASURED_PEAKS.json; 3 x forward FLOPs per sample"},
+                         "peak_source": f"bf16 burst peak: {peak_note}; 3 x forward FLOPs per sample"},
             "clocks": clk.summary(),
         }), flush=True)
 
@@ -507,8 +530,7 @@ def main() -> None:
            "d2h_bytes_per_step": int(sz.tally_words) * 8}
 
     if rank == 0:
-        peaks = _peaks()
-        f_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+        f_mhz, f_note = _peak("sm_max_mhz", 1965.0)
         n_sm = torch.cuda.get_device_properties(local).multi_processor_count
         e_int, e_bnd = STEPS_PER_PHOTON[a.workload]
         f_tot = e_int * F_INT + e_bnd * F_BND
@@ -532,7 +554,7 @@ def main() -> None:
                 "bound": "sfu" if s_tot / 16.0 >= f_tot / 128.0 else "fp32", "achieved": achieved / 1e9,
                 "peak": peak / 1e9, "unit": "Gphotons/s", "frac": achieved / peak,
                 "traffic": WALK_DRAM_BYTES.get(a.workload) if not a.photons else None,
-                "peak_source": f"issue roofline: {n_sm} SMs x {f_mhz:.0f} MHz (sm_max_mhz of MEASURED_PEAKS.json) / "
+                "peak_source": f"issue roofline: {n_sm} SMs x {f_mhz:.0f} MHz ({f_note}) / "
                                f"max(F/128, S/16) with F={f_tot:.0f} FP32 and S={s_tot:.0f} SFU ops per photon",
             },
             "clocks": clk.summary(),

@@ -297,11 +297,15 @@ TMC_B200_API int tmc_b200_gemm_bf16(const uint16_t *A, const uint16_t *B, const 
  *                (K / 64 a multiple of splits) into work (splits x M x N floats), then summed into
  *                D in a fixed order (deterministic); for long K and small M x N.
  * transpose:     Y = X^T for a rows x cols bf16 matrix.
- * colsum:        db[n] = sum_m dZ[m][n] (float32, overwritten).
+ * colsum:        db[n] = sum_m dZ[m][n] (float32, overwritten), in a fixed order (deterministic)
+ *                through `work`, which holds tmc_b200_nn_colsum_work(N) floats.
  * mse:           loss += scale * sum (pred - target)^2 over the first T of ld columns; dZ (bf16,
  *                optional) = 2 scale (pred - target), zero in the padded columns.
- * adam:          one Adam step (lr_t already bias-corrected) on float32 master weights, writing
- *                the bf16 copy wb and its transpose wt (each optional).
+ * adam:          one Adam step on float32 master weights, writing the bf16 copy wb and its
+ *                transpose wt (each optional). The bias-corrected step size is lr_t, or lr_dev[0]
+ *                when lr_dev (device memory) is given, so that a captured CUDA graph reads each
+ *                step's value; with avg given, avg = avg_beta avg + (1 - avg_beta) w afterwards
+ *                (Polyak averaging fused into the step, the same bits as the separate ema).
  * ema:           avg = beta avg + (1 - beta) w over n float32 values (Polyak averaging).
  * to_bf16:       wb = bf16(w) and wt = its transpose (each optional) for a rows x cols matrix.
  * status:        nonzero if a bounded tensor-core wait gave up since the last clear. */
@@ -316,13 +320,15 @@ TMC_B200_API int tmc_b200_nn_matmul_f32_splitk(const uint16_t *A, const uint16_t
                                                tmc_status *status);
 TMC_B200_API int tmc_b200_nn_transpose(const uint16_t *X, uint16_t *Y, int32_t rows, int32_t cols, void *stream,
                                        tmc_status *status);
-TMC_B200_API int tmc_b200_nn_colsum(const uint16_t *dZ, float *db, int32_t M, int32_t N, void *stream,
-                                    tmc_status *status);
+TMC_B200_API int tmc_b200_nn_colsum(const uint16_t *dZ, float *db, int32_t M, int32_t N, float *work,
+                                    void *stream, tmc_status *status);
+TMC_B200_API int32_t tmc_b200_nn_colsum_work(int32_t N);
 TMC_B200_API int tmc_b200_nn_mse(const float *pred, const float *target, uint16_t *dZ, float *loss, int32_t M,
                                  int32_t T, int32_t ld, float scale, void *stream, tmc_status *status);
 TMC_B200_API int tmc_b200_nn_adam(float *w, const float *g, float *m, float *v, int32_t rows, int32_t cols,
-                                  float lr_t, float b1, float b2, float eps, float weight_decay, uint16_t *wb,
-                                  uint16_t *wt, void *stream, tmc_status *status);
+                                  float lr_t, const float *lr_dev, float b1, float b2, float eps, float weight_decay,
+                                  uint16_t *wb, uint16_t *wt, float *avg, float avg_beta, void *stream,
+                                  tmc_status *status);
 TMC_B200_API int tmc_b200_nn_ema(const float *w, float *avg, int64_t n, float beta, void *stream, tmc_status *status);
 TMC_B200_API int tmc_b200_nn_to_bf16(const float *w, int32_t rows, int32_t cols, uint16_t *wb, uint16_t *wt,
                                      void *stream, tmc_status *status);

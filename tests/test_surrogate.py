@@ -111,9 +111,9 @@ def test_adam_transpose_and_colsum_kernels():
     s = torch.cuda.current_stream().cuda_stream
     import ctypes
 
-    S._call("tmc_b200_nn_adam", S._p(w), S._p(g), S._p(m), S._p(v), rows, cols, ctypes.c_float(0.01),
+    S._call("tmc_b200_nn_adam", S._p(w), S._p(g), S._p(m), S._p(v), rows, cols, ctypes.c_float(0.01), S._p(None),
             ctypes.c_float(0.9), ctypes.c_float(0.999), ctypes.c_float(1e-8), ctypes.c_float(0.0), S._p(wb),
-            S._p(wt), ctypes.c_void_p(s))
+            S._p(wt), S._p(None), ctypes.c_float(0.0), ctypes.c_void_p(s))
     torch.cuda.synchronize()
     mi = 0.1 * g
     vi = 0.001 * g * g
@@ -123,11 +123,81 @@ def test_adam_transpose_and_colsum_kernels():
     x = torch.randn(300, 70, device="cuda").bfloat16()
     y = torch.empty(70, 300, dtype=torch.bfloat16, device="cuda")
     S._call("tmc_b200_nn_transpose", S._p(x), S._p(y), 300, 70, ctypes.c_void_p(s))
+    work = torch.empty(tmc.lib().tmc_b200_nn_colsum_work(70), device="cuda")
     db = torch.empty(70, device="cuda")
-    S._call("tmc_b200_nn_colsum", S._p(x), S._p(db), 300, 70, ctypes.c_void_p(s))
+    S._call("tmc_b200_nn_colsum", S._p(x), S._p(db), 300, 70, S._p(work), ctypes.c_void_p(s))
     torch.cuda.synchronize()
     assert torch.equal(y, x.t())
     assert torch.allclose(db, x.float().sum(0), rtol=1e-5, atol=1e-4)
+
+
+def test_step_size_from_device_memory_and_fused_averaging_give_the_same_bits():
+    """Adam reading its step size from device memory, with the Polyak average fused, equals Adam
+    with the step size as an argument followed by the separate averaging pass, bit for bit; the
+    bias-gradient column sum is the same on every call (no atomics)."""
+    import ctypes
+
+    from tissuemc_b200 import surrogate as S
+
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rows, cols = 130, 257
+    gen = torch.Generator(device="cuda").manual_seed(9)
+    w = torch.randn(rows, cols, device="cuda", generator=gen)
+    g = torch.randn(rows, cols, device="cuda", generator=gen)
+    m = 0.1 * torch.randn(rows, cols, device="cuda", generator=gen)
+    v = torch.rand(rows, cols, device="cuda", generator=gen)
+    avg = torch.randn(rows, cols, device="cuda", generator=gen)
+    lr_dev = torch.tensor([3e-3], device="cuda")
+    a = [t.clone() for t in (w, m, v, avg)]
+    b = [t.clone() for t in (w, m, v, avg)]
+    wb_a, wb_b = (torch.empty(rows, cols, dtype=torch.bfloat16, device="cuda") for _ in range(2))
+    S._call("tmc_b200_nn_adam", S._p(a[0]), S._p(g), S._p(a[1]), S._p(a[2]), rows, cols, ctypes.c_float(0.0),
+            S._p(lr_dev), ctypes.c_float(0.9), ctypes.c_float(0.999), ctypes.c_float(1e-8), ctypes.c_float(1e-4),
+            S._p(wb_a), S._p(None), S._p(a[3]), ctypes.c_float(0.999), s)
+    S._call("tmc_b200_nn_adam", S._p(b[0]), S._p(g), S._p(b[1]), S._p(b[2]), rows, cols, ctypes.c_float(3e-3),
+            S._p(None), ctypes.c_float(0.9), ctypes.c_float(0.999), ctypes.c_float(1e-8), ctypes.c_float(1e-4),
+            S._p(wb_b), S._p(None), S._p(None), ctypes.c_float(0.0), s)
+    S._call("tmc_b200_nn_ema", S._p(b[0]), S._p(b[3]), rows * cols, ctypes.c_float(0.999), s)
+    torch.cuda.synchronize()
+    for x, y in zip(a, b, strict=True):
+        assert torch.equal(x, y)
+    assert torch.equal(wb_a, wb_b)
+    assert not torch.equal(a[3], avg)  # the average moved
+
+    dz = torch.randn(4096, 512, device="cuda", generator=gen).bfloat16()
+    work = torch.empty(tmc.lib().tmc_b200_nn_colsum_work(512), device="cuda")
+    sums = []
+    for _ in range(3):
+        db = torch.empty(512, device="cuda")
+        S._call("tmc_b200_nn_colsum", S._p(dz), S._p(db), 4096, 512, S._p(work), s)
+        sums.append(db)
+    torch.cuda.synchronize()
+    assert torch.equal(sums[0], sums[1]) and torch.equal(sums[0], sums[2])
+    assert torch.allclose(sums[0], dz.double().sum(0).float(), rtol=1e-4, atol=1e-3)
+
+
+def test_graph_captured_training_equals_host_launched_training():
+    """Training with the optimiser step captured once as a CUDA graph and replayed gives the same
+    weights and Adam moments, bit for bit, as launching every kernel from the host (the reported loss
+    is summed with atomics, so it agrees to rounding)."""
+    from tissuemc_b200 import surrogate as S
+
+    rng = np.random.default_rng(6)
+    X = rng.normal(size=(3 * 4096 + 100, S.N_FEAT))
+    Y = rng.normal(size=(len(X), S.N_OUT))
+    runs = []
+    for graph in (False, True):
+        ens = S.Ensemble(members=2, batch=4096, seed=5)
+        hist = ens.train(X, Y, epochs=3, lr=2e-3, ema=0.99, weight_decay=1e-4, graph=graph)
+        hist += ens.train(X[:4096], Y[:4096], epochs=2, lr=1e-3, graph=graph)  # Adam's step count carries over
+        torch.cuda.synchronize()
+        runs.append((hist, [[t.clone() for t in m.W + m.b + m.Wb + m.WT + m.mW + m.vW] for m in ens.members]))
+    (h0, p0), (h1, p1) = runs
+    np.testing.assert_allclose(h0, h1, rtol=1e-5)
+    for a, b in zip(p0, p1, strict=True):
+        for x, y in zip(a, b, strict=True):
+            assert torch.equal(x, y)
+    assert h0[2] < h0[0]  # and it trains
 
 
 @pytest.fixture(scope="module")

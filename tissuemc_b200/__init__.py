@@ -169,11 +169,14 @@ PROTOTYPES = {
     "tmc_b200_nn_matmul_f32_splitk": (ctypes.c_int, [ctypes.c_void_p] * 4 + [ctypes.c_int32] * 4 +
                                       [ctypes.c_void_p, _P(CStatus)]),
     "tmc_b200_nn_transpose": (ctypes.c_int, [ctypes.c_void_p] * 2 + [ctypes.c_int32] * 2 + [ctypes.c_void_p, _P(CStatus)]),
-    "tmc_b200_nn_colsum": (ctypes.c_int, [ctypes.c_void_p] * 2 + [ctypes.c_int32] * 2 + [ctypes.c_void_p, _P(CStatus)]),
+    "tmc_b200_nn_colsum": (ctypes.c_int, [ctypes.c_void_p] * 2 + [ctypes.c_int32] * 2 +
+                           [ctypes.c_void_p, ctypes.c_void_p, _P(CStatus)]),
+    "tmc_b200_nn_colsum_work": (ctypes.c_int32, [ctypes.c_int32]),
     "tmc_b200_nn_mse": (ctypes.c_int, [ctypes.c_void_p] * 4 + [ctypes.c_int32] * 3 + [ctypes.c_float, ctypes.c_void_p,
                                                                                         _P(CStatus)]),
-    "tmc_b200_nn_adam": (ctypes.c_int, [ctypes.c_void_p] * 4 + [ctypes.c_int32] * 2 + [ctypes.c_float] * 5 +
-                         [ctypes.c_void_p] * 3 + [_P(CStatus)]),
+    "tmc_b200_nn_adam": (ctypes.c_int, [ctypes.c_void_p] * 4 + [ctypes.c_int32] * 2 +
+                         [ctypes.c_float, ctypes.c_void_p] + [ctypes.c_float] * 4 + [ctypes.c_void_p] * 3 +
+                         [ctypes.c_float, ctypes.c_void_p, _P(CStatus)]),
     "tmc_b200_nn_status": (ctypes.c_int, [ctypes.c_int32]),
     "tmc_b200_nn_ema": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
                                        ctypes.c_void_p, _P(CStatus)]),

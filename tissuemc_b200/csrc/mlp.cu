@@ -137,8 +137,13 @@ __global__ void transpose_bf16_kernel(const __nv_bfloat16 *__restrict__ X, __nv_
         if (c0 + j < cols && r < rows) Y[static_cast<size_t>(c0 + j) * rows + r] = tile[threadIdx.x][j];
 }
 
-// db[n] = sum over rows of dZ[row][n] (one thread per column, rows strided over blockIdx.y).
-__global__ void colsum_kernel(const __nv_bfloat16 *__restrict__ dZ, float *__restrict__ db, int M, int N) {
+// Bias gradient db[n] = sum over rows of dZ[row][n], deterministically in two passes: block row y
+// of the first sums rows y, y + G, y + 2G, ... (G = kColsumGroups) of its 128 columns into
+// part[y][n]; the second adds the G partial sums of each column in a fixed order. No atomics, so a
+// training step gives the same bits every time it runs.
+constexpr int kColsumGroups = 128;
+
+__global__ void colsum_partial_kernel(const __nv_bfloat16 *__restrict__ dZ, float *__restrict__ part, int M, int N) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
     float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // four independent chains keep several loads in flight
@@ -148,7 +153,20 @@ __global__ void colsum_kernel(const __nv_bfloat16 *__restrict__ dZ, float *__res
         for (int u = 0; u < 4; ++u) s[u] += __bfloat162float(dZ[static_cast<size_t>(m + u * gridDim.y) * N + n]);
     }
     for (; m < M; m += gridDim.y) s[0] += __bfloat162float(dZ[static_cast<size_t>(m) * N + n]);
-    atomicAdd(&db[n], (s[0] + s[1]) + (s[2] + s[3]));
+    part[static_cast<size_t>(blockIdx.y) * N + n] = (s[0] + s[1]) + (s[2] + s[3]);
+}
+
+__global__ void colsum_final_kernel(const float *__restrict__ part, float *__restrict__ db, int N, int groups) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    int y = 0;
+    for (; y + 3 < groups; y += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s[u] += part[static_cast<size_t>(y + u) * N + n];
+    }
+    for (; y < groups; ++y) s[0] += part[static_cast<size_t>(y) * N + n];
+    db[n] = (s[0] + s[1]) + (s[2] + s[3]);
 }
 
 // Mean-squared error over the first T of ld columns: loss += scale * sum (p - t)^2 and
@@ -171,19 +189,30 @@ __global__ void mse_kernel(const float *__restrict__ pred, const float *__restri
     if ((threadIdx.x & 31) == 0 && l != 0.0f) atomicAdd(loss, l * scale);
 }
 
+// Polyak averaging of one value: avg = beta avg + (1 - beta) w, with its rounding pinned so that
+// the separate pass (ema_kernel) and the one fused into Adam give the same bits.
+__device__ __forceinline__ float polyak(float avg, float w, float beta) {
+    return __fmaf_rn(beta, avg, __fmul_rn(__fsub_rn(1.0f, beta), w));
+}
+
 // Adam on float32 master weights (rows x cols, row-major), writing the bf16 copy and its transpose.
+// The step size is lr_dev[0] when lr_dev is given (so that a captured graph reads the current
+// step's value), else lr_t; with avg given, the averaged weights are updated from the new ones.
 __global__ void adam_kernel(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
-                            float *__restrict__ v, int rows, int cols, float lr_t, float b1, float b2, float eps,
-                            float weight_decay, __nv_bfloat16 *wb, __nv_bfloat16 *wt) {
+                            float *__restrict__ v, int rows, int cols, float lr_t, const float *__restrict__ lr_dev,
+                            float b1, float b2, float eps, float weight_decay, __nv_bfloat16 *wb,
+                            __nv_bfloat16 *wt, float *__restrict__ avg, float avg_beta) {
     const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= static_cast<size_t>(rows) * cols) return;
+    const float lr = lr_dev ? __ldg(lr_dev) : lr_t;
     const float gi = g[i] + weight_decay * w[i];
     const float mi = b1 * m[i] + (1.0f - b1) * gi;
     const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
     m[i] = mi;
     v[i] = vi;
-    const float wi = w[i] - lr_t * mi / (sqrtf(vi) + eps);
+    const float wi = w[i] - lr * mi / (sqrtf(vi) + eps);
     w[i] = wi;
+    if (avg) avg[i] = polyak(avg[i], wi, avg_beta);
     const __nv_bfloat16 b = __float2bfloat16_rn(wi);
     if (wb) wb[i] = b;
     if (wt) {
@@ -203,7 +232,7 @@ __global__ void sum_splits_kernel(const float *__restrict__ work, float *__restr
 
 __global__ void ema_kernel(const float *__restrict__ w, float *__restrict__ avg, size_t n, float beta) {
     const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < n) avg[i] = beta * avg[i] + (1.0f - beta) * w[i];
+    if (i < n) avg[i] = polyak(avg[i], w[i], beta);
 }
 
 __global__ void to_bf16_kernel(const float *__restrict__ w, int rows, int cols, __nv_bfloat16 *wb,
@@ -434,17 +463,22 @@ int tmc_b200_nn_transpose(const uint16_t *X, uint16_t *Y, int32_t rows, int32_t 
     return launched(st);
 }
 
-int tmc_b200_nn_colsum(const uint16_t *dZ, float *db, int32_t M, int32_t N, void *stream, tmc_status *st) {
+int tmc_b200_nn_colsum(const uint16_t *dZ, float *db, int32_t M, int32_t N, float *work, void *stream,
+                       tmc_status *st) {
     put(st, TMC_OK, "");
-    if (!dZ || !db || M < 1 || N < 1) {
+    if (!dZ || !db || !work || M < 1 || N < 1) {
         put(st, TMC_BAD_ARGUMENT, "NULL argument or empty matrix");
         return TMC_BAD_ARGUMENT;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    cudaMemsetAsync(db, 0, sizeof(float) * N, s);
-    colsum_kernel<<<dim3((N + 127) / 128, 128), 128, 0, s>>>(reinterpret_cast<const __nv_bfloat16 *>(dZ), db, M, N);
+    const int groups = M < kColsumGroups ? M : kColsumGroups;
+    colsum_partial_kernel<<<dim3((N + 127) / 128, groups), 128, 0, s>>>(reinterpret_cast<const __nv_bfloat16 *>(dZ),
+                                                                      work, M, N);
+    colsum_final_kernel<<<(N + 127) / 128, 128, 0, s>>>(work, db, N, groups);
     return launched(st);
 }
+
+int32_t tmc_b200_nn_colsum_work(int32_t N) { return N < 1 ? 0 : kColsumGroups * N; }
 
 int tmc_b200_nn_mse(const float *pred, const float *target, uint16_t *dZ, float *loss, int32_t M, int32_t T,
                     int32_t ld, float scale, void *stream, tmc_status *st) {
@@ -459,9 +493,9 @@ int tmc_b200_nn_mse(const float *pred, const float *target, uint16_t *dZ, float 
     return launched(st);
 }
 
-int tmc_b200_nn_adam(float *w, const float *g, float *m, float *v, int32_t rows, int32_t cols, float lr_t, float b1,
-                     float b2, float eps, float weight_decay, uint16_t *wb, uint16_t *wt, void *stream,
-                     tmc_status *st) {
+int tmc_b200_nn_adam(float *w, const float *g, float *m, float *v, int32_t rows, int32_t cols, float lr_t,
+                     const float *lr_dev, float b1, float b2, float eps, float weight_decay, uint16_t *wb, uint16_t *wt,
+                     float *avg, float avg_beta, void *stream, tmc_status *st) {
     put(st, TMC_OK, "");
     if (!w || !g || !m || !v || rows < 1 || cols < 1) {
         put(st, TMC_BAD_ARGUMENT, "NULL argument or empty parameter");
@@ -469,8 +503,8 @@ int tmc_b200_nn_adam(float *w, const float *g, float *m, float *v, int32_t rows,
     }
     const size_t n = static_cast<size_t>(rows) * cols;
     adam_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        w, g, m, v, rows, cols, lr_t, b1, b2, eps, weight_decay, reinterpret_cast<__nv_bfloat16 *>(wb),
-        reinterpret_cast<__nv_bfloat16 *>(wt));
+        w, g, m, v, rows, cols, lr_t, lr_dev, b1, b2, eps, weight_decay, reinterpret_cast<__nv_bfloat16 *>(wb),
+        reinterpret_cast<__nv_bfloat16 *>(wt), avg, avg_beta);
     return launched(st);
 }
 

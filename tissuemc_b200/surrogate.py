@@ -164,7 +164,7 @@ class Member:
         while (batch // 64) % self.splits:
             self.splits -= 1
         self.work = torch.empty(self.splits * max(n * k for (k, n) in LAYER_DIMS), **f32)
-        self.step_count = 0
+        self.colsum_work = torch.empty(lib().tmc_b200_nn_colsum_work(max(n for (_, n) in LAYER_DIMS)), **f32)
         self.L = L
 
     def forward(self, X, rows: int, stream: int, Z_out=None):
@@ -194,23 +194,26 @@ class Member:
             prev_T = self.XT if li == 0 else self.HT[li - 1]
             _call("tmc_b200_nn_matmul_f32_splitk", _p(self.dZT[li]), _p(prev_T), _p(self.gW[li]), _p(self.work),
                   n, k, B, self.splits, s)
-            _call("tmc_b200_nn_colsum", _p(self.dZ[li]), _p(self.gb[li]), B, n, s)
+            _call("tmc_b200_nn_colsum", _p(self.dZ[li]), _p(self.gb[li]), B, n, _p(self.colsum_work), s)
             if li > 0:
                 _call("tmc_b200_nn_backward_data", _p(self.dZ[li]), _p(self.WT[li]), _p(self.Z[li - 1]),
                       _p(self.dZ[li - 1]), B, k, n, s)
 
-    def adam(self, stream: int, lr: float, b1=0.9, b2=0.999, eps=1e-8, wd=0.0):
-        self.step_count += 1
-        t = self.step_count
-        lr_t = lr * math.sqrt(1 - b2 ** t) / (1 - b1 ** t)
+    def adam(self, stream: int, lr_t: float = 0.0, lr_dev=None, b1=0.9, b2=0.999, eps=1e-8, wd=0.0, avg=None,
+             ema: float = 0.0):
+        """One Adam step of every parameter. The bias-corrected step size is lr_t, or the float32
+        in device memory at lr_dev (a captured graph reads each step's value there). With avg =
+        (weights, biases) float32 copies, the Polyak average avg = ema avg + (1 - ema) w follows the
+        step in the same kernel."""
         s = ctypes.c_void_p(stream)
+        aw, ab = avg if avg is not None else ([None] * self.L, [None] * self.L)
         for li, (k, n) in enumerate(LAYER_DIMS):
             _call("tmc_b200_nn_adam", _p(self.W[li]), _p(self.gW[li]), _p(self.mW[li]), _p(self.vW[li]), n, k,
-                  ctypes.c_float(lr_t), ctypes.c_float(b1), ctypes.c_float(b2), ctypes.c_float(eps),
-                  ctypes.c_float(wd), _p(self.Wb[li]), _p(self.WT[li]), s)
+                  ctypes.c_float(lr_t), _p(lr_dev), ctypes.c_float(b1), ctypes.c_float(b2), ctypes.c_float(eps),
+                  ctypes.c_float(wd), _p(self.Wb[li]), _p(self.WT[li]), _p(aw[li]), ctypes.c_float(ema), s)
             _call("tmc_b200_nn_adam", _p(self.b[li]), _p(self.gb[li]), _p(self.mb[li]), _p(self.vb[li]), 1, n,
-                  ctypes.c_float(lr_t), ctypes.c_float(b1), ctypes.c_float(b2), ctypes.c_float(eps),
-                  ctypes.c_float(0.0), _p(None), _p(None), s)
+                  ctypes.c_float(lr_t), _p(lr_dev), ctypes.c_float(b1), ctypes.c_float(b2), ctypes.c_float(eps),
+                  ctypes.c_float(0.0), _p(None), _p(None), _p(ab[li]), ctypes.c_float(ema), s)
 
 
 @dataclass
@@ -235,6 +238,7 @@ class Ensemble:
         self.members = [Member(batch, seed * 1000 + i, device) for i in range(members)]
         self.norm: Norm | None = None
         self.history: list[float] = []
+        self.step_count = 0  # optimiser steps taken (Adam's bias correction continues across train calls)
 
     def _x(self, X: np.ndarray):
         t = self.torch
@@ -243,11 +247,19 @@ class Ensemble:
         return t.from_numpy(Xn).to(self.dev).to(t.bfloat16)
 
     def train(self, X: np.ndarray, Y: np.ndarray, epochs: int, lr: float = 1e-3, seed: int = 0,
-              lr_final: float = 1e-5, ema: float = 0.0, weight_decay: float = 0.0) -> list[float]:
+              lr_final: float = 1e-5, ema: float = 0.0, weight_decay: float = 0.0, graph: bool = True) -> list[float]:
         """Adam with a cosine learning-rate decay; returns the mean training loss per epoch. With
         ema > 0 every member also keeps an exponential moving average of its weights (Polyak
-        averaging, avg = ema avg + (1 - ema) w after each step), which replaces the weights at the
-        end."""
+        averaging, avg = ema avg + (1 - ema) w after each step, in the Adam kernel), which replaces
+        the weights at the end.
+
+        One optimiser step of the whole ensemble (batch gathers, forward, backward, Adam and
+        averaging: about 50 launches per member) runs once from the host and is then captured as a
+        CUDA graph that every later step replays; each step's batch indices and step size reach the
+        graph through device buffers written before the replay. graph=False launches every kernel
+        from the host instead. Both give the same weights bit for bit: no kernel that writes them
+        depends on the order in which threads finish (only the reported loss is summed with
+        atomics)."""
         t = self.torch
         self.norm = Norm.fit(X, Y)
         Xd = self._x(X)
@@ -256,43 +268,63 @@ class Ensemble:
         steps = n // self.B
         if steps < 1:
             raise ValueError(f"need at least one full batch of {self.B} samples")
-        stream = t.cuda.current_stream().cuda_stream
         gen = t.Generator(device=self.dev).manual_seed(seed)
         scale = 1.0 / (self.B * N_OUT)
         total = epochs * steps
+        b1, b2 = 0.9, 0.999
         xb = t.empty(self.B, K_IN, dtype=t.bfloat16, device=self.dev)
         yb = t.empty(self.B, N_OUT, dtype=t.float32, device=self.dev)
-        k = 0
-        t_start, t_end = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
-        t_start.record()
-        avg = []
+        idx = t.empty(len(self.members), self.B, dtype=t.int64, device=self.dev)  # this step's rows, per member
+        lr_dev = t.zeros(1, dtype=t.float32, device=self.dev)  # this step's bias-corrected step size
+        acc = t.zeros(1, dtype=t.float32, device=self.dev)  # the epoch's summed loss
+        avg = [None] * len(self.members)
         if ema > 0:
             avg = [([w.clone() for w in m.W], [b.clone() for b in m.b]) for m in self.members]
+
+        def one_step():
+            stream = t.cuda.current_stream().cuda_stream  # the capturing stream during capture
+            for m, rows, avg_m in zip(self.members, idx, avg, strict=True):
+                t.index_select(Xd, 0, rows, out=xb)
+                t.index_select(Yd, 0, rows, out=yb)
+                m.forward(xb, self.B, stream)
+                m.backward(xb, yb, stream, scale)
+                m.adam(stream, lr_dev=lr_dev, wd=weight_decay, avg=avg_m, ema=ema)
+                acc.add_(m.loss)
+
+        step_graph = None
+        t_start, t_end = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
+        timed_from = min(1, total - 1)  # the first step (one-time set-up, then the capture) is untimed
+        k = 0
         for _ in range(epochs):
-            perms = [t.randperm(n, generator=gen, device=self.dev) for _ in self.members]
-            acc = t.zeros(1, dtype=t.float32, device=self.dev)
+            perm = t.stack([t.randperm(n, generator=gen, device=self.dev) for _ in self.members])
+            acc.zero_()
             for s in range(steps):
                 lr_k = lr_final + 0.5 * (lr - lr_final) * (1 + math.cos(math.pi * k / total))
-                for mi, (m, perm) in enumerate(zip(self.members, perms, strict=True)):
-                    idx = perm[s * self.B:(s + 1) * self.B]
-                    t.index_select(Xd, 0, idx, out=xb)
-                    t.index_select(Yd, 0, idx, out=yb)
-                    m.forward(xb, self.B, stream)
-                    m.backward(xb, yb, stream, scale)
-                    m.adam(stream, lr_k, wd=weight_decay)
-                    acc += m.loss
-                    if avg:
-                        aw, ab = avg[mi]
-                        for p, q in zip(m.W + m.b, aw + ab, strict=True):
-                            _call("tmc_b200_nn_ema", _p(p), _p(q), p.numel(), ctypes.c_float(ema),
-                                  ctypes.c_void_p(stream))
+                self.step_count += 1
+                c = self.step_count
+                lr_dev.fill_(lr_k * math.sqrt(1 - b2 ** c) / (1 - b1 ** c))
+                idx.copy_(perm[:, s * self.B:(s + 1) * self.B])
+                if k == timed_from:
+                    t_start.record()
+                if step_graph is not None:
+                    step_graph.replay()
+                else:
+                    one_step()
+                    if graph and total > 1:
+                        step_graph = t.cuda.CUDAGraph()
+                        with t.cuda.graph(step_graph):
+                            one_step()
                 k += 1
             self.history.append(float(acc.item()) / (steps * len(self.members)))
         t_end.record()
         t_end.synchronize()
-        self.last_step_ms = t_start.elapsed_time(t_end) / max(1, total)  # device time per optimiser step
-        for m, (aw, ab) in zip(self.members, avg):
-            for li, (w, b) in enumerate(zip(aw, ab, strict=True)):
+        self.last_step_ms = t_start.elapsed_time(t_end) / (total - timed_from)  # device time per optimiser step
+        del step_graph
+        stream = t.cuda.current_stream().cuda_stream
+        for m, avg_m in zip(self.members, avg, strict=True):
+            if avg_m is None:
+                continue
+            for li, (w, b) in enumerate(zip(*avg_m, strict=True)):
                 m.W[li].copy_(w)
                 m.b[li].copy_(b)
                 n_out, k_in = LAYER_DIMS[li][1], LAYER_DIMS[li][0]
