@@ -255,11 +255,11 @@ class Ensemble:
 
         One optimiser step of the whole ensemble (batch gathers, forward, backward, Adam and
         averaging: about 50 launches per member) runs once from the host and is then captured as a
-        CUDA graph that every later step replays; each step's batch indices and step size reach the
-        graph through device buffers written before the replay. graph=False launches every kernel
-        from the host instead. Both give the same weights bit for bit: no kernel that writes them
-        depends on the order in which threads finish (only the reported loss is summed with
-        atomics)."""
+        CUDA graph, one independent branch per member, that every later step replays; each step's
+        batch indices and step size reach the graph through device buffers written before the
+        replay. graph=False launches every kernel from the host, one member after the other. Both
+        give the same weights bit for bit: no kernel that writes them depends on the order in which
+        threads finish (only the reported loss is summed with atomics)."""
         t = self.torch
         self.norm = Norm.fit(X, Y)
         Xd = self._x(X)
@@ -272,24 +272,41 @@ class Ensemble:
         scale = 1.0 / (self.B * N_OUT)
         total = epochs * steps
         b1, b2 = 0.9, 0.999
-        xb = t.empty(self.B, K_IN, dtype=t.bfloat16, device=self.dev)
-        yb = t.empty(self.B, N_OUT, dtype=t.float32, device=self.dev)
-        idx = t.empty(len(self.members), self.B, dtype=t.int64, device=self.dev)  # this step's rows, per member
+        nm = len(self.members)
+        xb = [t.empty(self.B, K_IN, dtype=t.bfloat16, device=self.dev) for _ in range(nm)]
+        yb = [t.empty(self.B, N_OUT, dtype=t.float32, device=self.dev) for _ in range(nm)]
+        idx = t.empty(nm, self.B, dtype=t.int64, device=self.dev)  # this step's rows, per member
         lr_dev = t.zeros(1, dtype=t.float32, device=self.dev)  # this step's bias-corrected step size
-        acc = t.zeros(1, dtype=t.float32, device=self.dev)  # the epoch's summed loss
-        avg = [None] * len(self.members)
+        acc = t.zeros(nm, dtype=t.float32, device=self.dev)  # each member's summed loss over the epoch
+        avg = [None] * nm
         if ema > 0:
             avg = [([w.clone() for w in m.W], [b.clone() for b in m.b]) for m in self.members]
+        # with the graph, each member's kernels go to a stream of its own, so the captured step has one
+        # independent branch per member and the small products of the members run side by side
+        branches = [t.cuda.Stream(device=self.dev) for _ in range(nm)] if graph else []
+
+        def member_step(mi):
+            m = self.members[mi]
+            stream = t.cuda.current_stream().cuda_stream  # a capturing stream during capture
+            t.index_select(Xd, 0, idx[mi], out=xb[mi])
+            t.index_select(Yd, 0, idx[mi], out=yb[mi])
+            m.forward(xb[mi], self.B, stream)
+            m.backward(xb[mi], yb[mi], stream, scale)
+            m.adam(stream, lr_dev=lr_dev, wd=weight_decay, avg=avg[mi], ema=ema)
+            acc[mi:mi + 1].add_(m.loss)
 
         def one_step():
-            stream = t.cuda.current_stream().cuda_stream  # the capturing stream during capture
-            for m, rows, avg_m in zip(self.members, idx, avg, strict=True):
-                t.index_select(Xd, 0, rows, out=xb)
-                t.index_select(Yd, 0, rows, out=yb)
-                m.forward(xb, self.B, stream)
-                m.backward(xb, yb, stream, scale)
-                m.adam(stream, lr_dev=lr_dev, wd=weight_decay, avg=avg_m, ema=ema)
-                acc.add_(m.loss)
+            if not branches:
+                for mi in range(nm):
+                    member_step(mi)
+                return
+            main = t.cuda.current_stream()
+            for mi, br in enumerate(branches):
+                br.wait_stream(main)
+                with t.cuda.stream(br):
+                    member_step(mi)
+            for br in branches:
+                main.wait_stream(br)
 
         step_graph = None
         t_start, t_end = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
@@ -315,7 +332,7 @@ class Ensemble:
                         with t.cuda.graph(step_graph):
                             one_step()
                 k += 1
-            self.history.append(float(acc.item()) / (steps * len(self.members)))
+            self.history.append(float(acc.sum().item()) / (steps * nm))
         t_end.record()
         t_end.synchronize()
         self.last_step_ms = t_start.elapsed_time(t_end) / (total - timed_from)  # device time per optimiser step
