@@ -44,8 +44,6 @@ class SweepFail : public std::runtime_error {
                                                 std::to_string(__LINE__) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-constexpr uint32_t kPermCandidates[] = {2654435761u, 2246822519u, 3266489917u, 668265263u, 374761393u};
-
 void put(tmc_status *st, int code, const std::string &m) {
     if (!st) return;
     st->code = code;
@@ -309,19 +307,7 @@ uint32_t fill_blob(SweepGraph &g, const tmc_sweep_config *cfgs, int n) {
     }
     if (total >= 0xFFFFFFFFull) throw ConfigFailure("too many work items; raise item_photons");
     prefix[n] = static_cast<uint32_t>(total);
-    SweepHeader h{static_cast<uint32_t>(n), static_cast<uint32_t>(total), 1u, item};
-    for (uint32_t p : kPermCandidates) {  // a multiplier coprime with the item count
-        uint64_t a = p % total, b = total;
-        while (b) {
-            const uint64_t t = a % b;
-            a = b;
-            b = t;
-        }
-        if (a == 1 && total > 1) {
-            h.perm = static_cast<uint32_t>(p % total);
-            break;
-        }
-    }
+    const SweepHeader h{static_cast<uint32_t>(n), static_cast<uint32_t>(total), sweep_perm(total), item};
     std::memcpy(g.h_blob, &h, sizeof h);
     return h.total_items;
 }

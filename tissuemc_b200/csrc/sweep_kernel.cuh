@@ -18,6 +18,7 @@
 #pragma once
 
 #include "walk_step.cuh"
+#include "work_queue.cuh"
 
 namespace tmc {
 
@@ -156,19 +157,8 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                     if (static_cast<int>(lane) == leader) idx = atomicAdd(P.item_counter, 1u);
                     idx = __shfl_sync(0xffffffffu, idx, leader);
                     if (idx < H.total_items) {
-                        const uint32_t j = static_cast<uint32_t>(
-                            (static_cast<uint64_t>(idx) * H.perm) % H.total_items);
-                        uint32_t lo = 0u, hi = H.n_cfg;  // the c with prefix[c] <= j < prefix[c + 1]
-                        while (hi - lo > 1u) {
-                            const uint32_t mid = (lo + hi) >> 1;
-                            if (P.prefix[mid] <= j) lo = mid;
-                            else hi = mid;
-                        }
-                        const uint32_t first = (j - P.prefix[lo]) * H.item_photons;
-                        const uint32_t left = P.cfgs[lo].photons - first;
-                        it_cfg = lo;
-                        it_next = first;
-                        it_end = first + (left < H.item_photons ? left : H.item_photons);
+                        sweep_item(idx, H.total_items, H.perm, H.item_photons, H.n_cfg, P.prefix,
+                                   [&](uint32_t c) { return P.cfgs[c].photons; }, it_cfg, it_next, it_end);
                         continue;
                     }
                     items_done = true;
@@ -188,8 +178,7 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                 C.nl = cf.nl;
                 C.layers = P.layers + cf.layer_base;
                 C.t = P.tally + static_cast<size_t>(it_cfg) * static_cast<size_t>(P.stride);
-                const int batch = static_cast<int>(id < cf.plan_bnd ? id / (cf.plan_base + 1u)
-                                                                    : cf.plan_extra + (id - cf.plan_bnd) / cf.plan_base);
+                const int batch = batch_of(id, cf.plan_base, cf.plan_extra, cf.plan_bnd);
                 launch(L, C, id, batch, cf.launch_w);
                 alive = true;
             }

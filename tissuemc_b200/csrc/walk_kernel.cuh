@@ -3,6 +3,7 @@
 #pragma once
 
 #include "walk_step.cuh"
+#include "work_queue.cuh"
 
 namespace tmc {
 
@@ -169,7 +170,7 @@ __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P
     const uint32_t n_photons = static_cast<uint32_t>(P.photons);  // at most 2^31 (validated)
     const uint32_t chunk = static_cast<uint32_t>(P.chunk);
 
-    uint32_t pool_next = 0u, pool_end = 0u;  // warp-uniform photon-id pool
+    WarpPool pool;                           // warp-uniform photon-id pool
     unsigned ex_mask = 0u;                   // warp-uniform: lanes with no photon left to take
     bool alive = false;
     Lane L;
@@ -180,27 +181,18 @@ __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P
         if (need) {
             const uint32_t n = static_cast<uint32_t>(__popc(need));
             const uint32_t rank = static_cast<uint32_t>(__popc(need & lt_mask));
-            const uint32_t avail = pool_end - pool_next;
-            uint32_t my;
-            if (avail >= n) {
-                my = pool_next + rank;
-                pool_next += n;
-            } else {
+            uint32_t base = 0u;
+            if (pool.must_claim(n)) {  // one lane claims the next chunk for the warp
                 const int leader = __ffs(need) - 1;
-                uint32_t base = 0u;
                 if (static_cast<int>(lane) == leader) base = atomicAdd(P.counter, chunk);
                 base = __shfl_sync(0xffffffffu, base, leader);
-                my = rank < avail ? pool_next + rank : base + (rank - avail);
-                pool_next = base + (n - avail);
-                pool_end = base + chunk;
             }
+            const uint32_t my = pool.take(n, rank, base, chunk);
             const bool mine = (need >> lane) & 1u;
             ex_mask |= __ballot_sync(0xffffffffu, mine && my >= n_photons);
             if (mine && my < n_photons) {
                 const uint32_t id = P.id_base + my;  // the run's photon id: its stream and its batch
-                const int batch = static_cast<int>(id < P.plan_bnd ? id / (P.plan_base + 1u)
-                                                                   : P.plan_extra + (id - P.plan_bnd) / P.plan_base);
-                launch(L, C, id, batch, P.launch_w);
+                launch(L, C, id, batch_of(id, P.plan_base, P.plan_extra, P.plan_bnd), P.launch_w);
                 alive = true;
             }
         }
