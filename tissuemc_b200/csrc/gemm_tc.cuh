@@ -1,80 +1,64 @@
 // D = A * B^T on the 5th-generation tensor cores (tcgen05), BF16 operands, FP32 accumulation in
 // tensor memory, with a fused epilogue. A is M x K and B is N x K, both row-major with K
-// contiguous (K-major); K is a multiple of 64. One CTA of 128 threads computes a 128 x BN tile
-// over the K range of its blockIdx.z (split-K: each z covers K / gridDim.z, a multiple of 64):
+// contiguous (K-major), 16-byte aligned; K is a multiple of 64. One CTA of four warps computes a
+// 128 x BN tile over the K range of its blockIdx.z (split-K: each z covers K / gridDim.z, a
+// multiple of 64):
 //
-//   two shared-memory stages hold 64-wide K slices of A and B in the 128-byte-swizzled K-major
-//   layout (umma.cuh). Each thread keeps the next slice's global loads in flight in registers
-//   (issued together, before the current slice's MMAs), then stores them into the stage whose
-//   MMAs (two slices back) have completed, fences them for the tensor core's async proxy and
-//   synchronises; thread 0 issues four tcgen05.mma (K = 16 each) into the TMEM accumulator and
-//   commits them to that stage's mbarrier. Every wait is bounded: one that runs out records an
-//   error in *status and the results are discarded by the host.
+//   warp 0 (the producer) streams 64-wide K slices of A and B into a ring of kGemmStages
+//   shared-memory stages with tiled TMA loads (cp.async.bulk.tensor, 128-byte swizzle: the layout
+//   the MMA descriptors read, umma.cuh), each stage's mbarrier counting the bytes in; warp 1 (the
+//   issuer) waits for a stage, issues its four tcgen05.mma (K = 16 each) into the TMEM accumulator
+//   and commits them to the stage's "empty" mbarrier, which hands the stage back to the producer;
+//   a last commit marks the accumulator complete. Rows past M or N arrive as zeros. Every wait is
+//   bounded: one that runs out records an error in *status (the host discards the results), and
+//   the producer waits (bounded) for every load it issued before the CTA may exit.
 //   The epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31, i.e.
 //   output rows m0 + 32w + lane), applies the epilogue functor (given the split index) and writes
 //   global memory.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include "umma.cuh"
 
 namespace tmc {
 
-constexpr int kGemmBM = 128, kGemmBK = 64, kGemmThreads = 128;
+constexpr int kGemmBM = 128, kGemmBK = 64, kGemmThreads = 128, kGemmStages = 3;
 constexpr uint32_t kGemmWaitLimit = 1u << 24;  // mbarrier polls before a wait gives up
 
 template <int BN> struct GemmSmem {
     static constexpr int a_bytes = kGemmBM * 128;  // 128 rows x 64 bf16
     static constexpr int b_bytes = BN * 128;
     static constexpr int stage_bytes = a_bytes + b_bytes;
-    static constexpr int bytes = 1024 /*alignment slack*/ + 2 * stage_bytes + 64;
-};
-
-// Global loads of one 64-wide K slice of a K-major bf16 matrix: rows [row0, row0 + ROWS), 8
-// 16-byte units per row, ROWS * 8 / kGemmThreads units per thread (issued together).
-template <int ROWS> struct SliceRegs {
-    static constexpr int per_thread = ROWS * 8 / kGemmThreads;
-    uint4 v[per_thread];
-
-    __device__ __forceinline__ void load(const __nv_bfloat16 *X, int ld, int nrows_total, int row0, int k0) {
-#pragma unroll
-        for (int i = 0; i < per_thread; ++i) {
-            const int idx = threadIdx.x + i * kGemmThreads;
-            const int r = idx >> 3, c = idx & 7;
-            v[i] = make_uint4(0u, 0u, 0u, 0u);
-            if (row0 + r < nrows_total)
-                v[i] = *reinterpret_cast<const uint4 *>(X + static_cast<size_t>(row0 + r) * ld + k0 + c * 8);
-        }
-    }
-    __device__ __forceinline__ void store(unsigned char *tile) const {
-#pragma unroll
-        for (int i = 0; i < per_thread; ++i) {
-            const int idx = threadIdx.x + i * kGemmThreads;
-            const int r = idx >> 3, c = idx & 7;
-            *reinterpret_cast<uint4 *>(tile + r * 128 + ((c ^ (r & 7)) << 4)) = v[i];
-        }
-    }
+    // alignment slack, the stages, then 2 x kGemmStages + 1 mbarriers and the TMEM address
+    static constexpr int bytes = 1024 + kGemmStages * stage_bytes + 128;
 };
 
 // Epilogue functor interface: operator()(split, row, col0, v[8]) for 8 consecutive columns of one
 // row (col0 is a multiple of 8; columns at or beyond N must be ignored by the functor).
 template <int BN, class Epi>
-__global__ void __launch_bounds__(kGemmThreads) gemm_tc_kernel(const __nv_bfloat16 *__restrict__ A,
-                                                              const __nv_bfloat16 *__restrict__ B, int M, int N,
+__global__ void __launch_bounds__(kGemmThreads) gemm_tc_kernel(const __grid_constant__ CUtensorMap tma_a,
+                                                              const __grid_constant__ CUtensorMap tma_b, int M, int N,
                                                               int K, Epi epi, int *status) {
+    static_assert(GemmSmem<BN>::a_bytes % 1024 == 0 && GemmSmem<BN>::b_bytes % 1024 == 0, "1024-byte tiles");
     extern __shared__ unsigned char gsm_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(gsm_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-    uint64_t *bar = reinterpret_cast<uint64_t *>(base + 2 * GemmSmem<BN>::stage_bytes);  // [2]
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 2);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + kGemmStages * GemmSmem<BN>::stage_bytes);
+    uint64_t *empty = full + kGemmStages;
+    uint64_t *acc_bar = empty + kGemmStages;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_bar + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * kGemmBM, n0 = blockIdx.x * BN;
     if (warp == 0) tmem_alloc(tmem_slot, BN);
     if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int s = 0; s < kGemmStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(acc_bar, 1);
     }
     tc_fence_before();
     __syncthreads();
@@ -84,41 +68,56 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_tc_kernel(const __nv_bfloat
 
     const int kt_n = K / kGemmBK / static_cast<int>(gridDim.z);  // K slices of this split
     const int kt0 = static_cast<int>(blockIdx.z) * kt_n;
-    SliceRegs<kGemmBM> ra;
-    SliceRegs<BN> rb;
-    ra.load(A, K, M, m0, kt0 * kGemmBK);
-    rb.load(B, K, N, n0, kt0 * kGemmBK);
     bool ok = true;
-    for (int kt = 0; kt < kt_n; ++kt) {
-        const int s = kt & 1;
-        unsigned char *sa = base + s * GemmSmem<BN>::stage_bytes;
-        unsigned char *sb = sa + GemmSmem<BN>::a_bytes;
-        // the stage was last read by the MMAs of slice kt - 2
-        if (kt >= 2 && ok && !mbar_wait(&bar[s], static_cast<uint32_t>(((kt - 2) >> 1) & 1), kGemmWaitLimit)) {
-            ok = false;
-            atomicExch(status, 1);
+    if (warp == 0) {
+        // ---- producer: the whole warp walks the ring, lane 0 issues
+        int issued = 0;
+        for (int kt = 0; kt < kt_n; ++kt) {
+            const int s = kt % kGemmStages;
+            // the stage was last read by the MMAs of slice kt - kGemmStages
+            if (kt >= kGemmStages &&
+                !mbar_wait(&empty[s], static_cast<uint32_t>((kt / kGemmStages - 1) & 1), kGemmWaitLimit)) {
+                ok = false;
+                break;
+            }
+            if (lane == 0) {
+                unsigned char *sa = base + s * GemmSmem<BN>::stage_bytes;
+                mbar_arrive_expect_tx(&full[s], GemmSmem<BN>::stage_bytes);
+                tma_load_2d(sa, &tma_a, (kt0 + kt) * kGemmBK, m0, &full[s]);
+                tma_load_2d(sa + GemmSmem<BN>::a_bytes, &tma_b, (kt0 + kt) * kGemmBK, n0, &full[s]);
+            }
+            __syncwarp();
+            issued = kt + 1;
         }
-        ra.store(sa);
-        rb.store(sb);
-        fence_async_smem();
-        __syncthreads();
-        if (kt + 1 < kt_n) {  // the next slice's loads fly while this slice's MMAs run
-            ra.load(A, K, M, m0, (kt0 + kt + 1) * kGemmBK);
-            rb.load(B, K, N, n0, (kt0 + kt + 1) * kGemmBK);
-        }
-        if (threadIdx.x == 0) {
+        // every load issued has landed before the CTA can end (the last phase of each stage)
+        for (int kt = issued > kGemmStages ? issued - kGemmStages : 0; kt < issued; ++kt)
+            if (!mbar_wait(&full[kt % kGemmStages], static_cast<uint32_t>((kt / kGemmStages) & 1), kGemmWaitLimit))
+                ok = false;
+    } else if (warp == 1) {
+        // ---- issuer: the whole warp waits, lane 0 issues the MMAs and the commits
+        for (int kt = 0; kt < kt_n; ++kt) {
+            const int s = kt % kGemmStages;
+            if (!mbar_wait(&full[s], static_cast<uint32_t>((kt / kGemmStages) & 1), kGemmWaitLimit)) {
+                ok = false;
+                break;
+            }
             tc_fence_after();
-            const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
+            if (lane == 0) {
+                const uint32_t a0 = smem_u32(base + s * GemmSmem<BN>::stage_bytes);
+                const uint32_t b0 = a0 + GemmSmem<BN>::a_bytes;
 #pragma unroll
-            for (int kk = 0; kk < kGemmBK / 16; ++kk)  // 16 bf16 = 32 bytes further along K
-                umma_bf16(tmem_d, umma_desc_sw128(a0 + kk * 32), umma_desc_sw128(b0 + kk * 32), idesc,
-                          (kt > 0 || kk > 0) ? 1u : 0u);
-            umma_commit(&bar[s]);
+                for (int kk = 0; kk < kGemmBK / 16; ++kk)  // 16 bf16 = 32 bytes further along K
+                    umma_bf16(tmem_d, umma_desc_sw128(a0 + kk * 32), umma_desc_sw128(b0 + kk * 32), idesc,
+                              (kt > 0 || kk > 0) ? 1u : 0u);
+                umma_commit(&empty[s]);
+            }
+            __syncwarp();
         }
+        if (lane == 0) umma_commit(acc_bar);  // arrives when every MMA issued above has completed
+        __syncwarp();
     }
-    // the last commit completes when every MMA of the tile has
-    const int last = kt_n - 1;
-    if (ok && !mbar_wait(&bar[last & 1], static_cast<uint32_t>((last >> 1) & 1), kGemmWaitLimit)) {
+    if (!ok && lane == 0) atomicExch(status, 1);
+    if (ok && !mbar_wait(acc_bar, 0u, kGemmWaitLimit)) {
         ok = false;
         atomicExch(status, 1);
     }

@@ -6,8 +6,10 @@
 // do not synchronise (so a training step can be captured in a CUDA graph); a bounded tensor-core
 // wait that gives up sets a per-device status word read by tmc_b200_nn_status.
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstdio>
@@ -23,9 +25,9 @@ namespace tmc {
 namespace {
 
 constexpr int kBN = 128;
-// two stages of 32 KB plus slack: at most three CTAs per SM, i.e. 3 x 128 of the 512 TMEM columns
-constexpr int kGemmSmemRequest = 68 * 1024;
-static_assert(GemmSmem<128>::bytes <= kGemmSmemRequest, "GEMM shared memory");
+// three stages of 32 KB plus slack: two CTAs per SM, i.e. 2 x 128 of the 512 TMEM columns
+constexpr int kGemmSmemRequest = GemmSmem<kBN>::bytes;
+static_assert(2 * kGemmSmemRequest <= 227 * 1024, "two GEMM CTAs per SM");
 
 __device__ __forceinline__ float gelu(float x) { return gelu_tanh(x); }
 __device__ __forceinline__ float gelu_grad(float x) { return gelu_tanh_grad(x); }
@@ -314,6 +316,21 @@ template <class Epi> void set_smem_attr() {
     cudaFuncSetAttribute(gemm_tc_kernel<kBN, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmemRequest);
 }
 
+// cuTensorMapEncodeTiled, from the driver through the runtime (no link against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 g_encode_tiled = nullptr;
+
+// Tensor map of a rows x K bf16 matrix (K contiguous) read in boxes of 64 (K) x box_rows, with the
+// 128-byte swizzle of the MMA operand tiles; rows past the end read as zeros.
+bool encode_operand(CUtensorMap *map, const void *ptr, int rows, int K, int box_rows) {
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(K), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(K) * 2u};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(kGemmBK), static_cast<cuuint32_t>(box_rows)};
+    const cuuint32_t elem[2] = {1u, 1u};
+    return g_encode_tiled(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, elem,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Common checks and the launch of one tensor-core GEMM (asynchronous).
 template <class Epi>
 int launch_gemm(const void *A, const void *B, int M, int N, int K, const Epi &epi, void *stream, tmc_status *st,
@@ -330,6 +347,10 @@ int launch_gemm(const void *A, const void *B, int M, int N, int K, const Epi &ep
         put(st, TMC_BAD_CONFIG, "split-K needs K / 64 to be a multiple of the number of splits");
         return TMC_BAD_CONFIG;
     }
+    if (reinterpret_cast<uintptr_t>(A) % 16 != 0 || reinterpret_cast<uintptr_t>(B) % 16 != 0) {
+        put(st, TMC_BAD_ARGUMENT, "tensor-core GEMM operands must be 16-byte aligned");
+        return TMC_BAD_ARGUMENT;
+    }
     const int dev = current_device();
     std::lock_guard<std::mutex> lock(g_mu);
     int *status = status_word(dev);
@@ -337,15 +358,32 @@ int launch_gemm(const void *A, const void *B, int M, int N, int K, const Epi &ep
         put(st, TMC_NO_DEVICE, "no usable CUDA device found");
         return TMC_NO_DEVICE;
     }
+    if (!g_encode_tiled) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            cudaGetLastError();
+            put(st, TMC_CUDA_ERROR, "the CUDA driver does not provide cuTensorMapEncodeTiled");
+            return TMC_CUDA_ERROR;
+        }
+        g_encode_tiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
     if (!g_attr[dev]) {
         set_smem_attr<EpiF32>();
         set_smem_attr<EpiFwd>();
         set_smem_attr<EpiBwd>();
         g_attr[dev] = true;
     }
+    CUtensorMap ta, tb;
+    if (!encode_operand(&ta, A, M, K, kGemmBM) || !encode_operand(&tb, B, N, K, kBN)) {
+        put(st, TMC_BAD_ARGUMENT, "tensor-core GEMM operands do not fit a TMA tensor map");
+        return TMC_BAD_ARGUMENT;
+    }
     const dim3 grid((N + kBN - 1) / kBN, (M + kGemmBM - 1) / kGemmBM, splits);
     gemm_tc_kernel<kBN, Epi><<<grid, kGemmThreads, kGemmSmemRequest, static_cast<cudaStream_t>(stream)>>>(
-        static_cast<const __nv_bfloat16 *>(A), static_cast<const __nv_bfloat16 *>(B), M, N, K, epi, status);
+        ta, tb, M, N, K, epi, status);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         put(st, TMC_CUDA_ERROR, std::string("CUDA error launching the tensor-core GEMM: ") + cudaGetErrorString(e));

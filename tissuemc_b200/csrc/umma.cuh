@@ -145,6 +145,19 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
                  : "memory");
 }
 
+// Tiled TMA load (cp.async.bulk.tensor, 2-D, no multicast) of the box at element coordinates
+// (x, y) of the tensor map `tmap` (a __grid_constant__ kernel parameter) into this CTA's shared
+// memory, swizzled as the map says; the mbarrier's transaction count drops by the box's bytes when
+// it has landed (rows outside the tensor arrive as zeros). x times the element size must be a
+// multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_2d(void *smem_dst, const void *tmap, int x, int y, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(smem_dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
 // Bulk copy (the TMA engine, untiled) of `bytes` from global to this CTA's shared memory; the
 // mbarrier's transaction count drops by `bytes` when the data has landed. Both addresses 16-byte
 // aligned, bytes a multiple of 16.
