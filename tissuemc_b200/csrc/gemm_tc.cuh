@@ -12,9 +12,9 @@
 //   a last commit marks the accumulator complete. Rows past M or N arrive as zeros. Every wait is
 //   bounded: one that runs out records an error in *status (the host discards the results), and
 //   the producer waits (bounded) for every load it issued before the CTA may exit.
-//   The epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31, i.e.
-//   output rows m0 + 32w + lane), applies the epilogue functor (given the split index) and writes
-//   global memory.
+//   The epilogue reads the accumulator with tcgen05.ld, 32 columns per load (warp w owns TMEM
+//   lanes 32w..32w+31, i.e. output rows m0 + 32w + lane), applies the epilogue functor (given the
+//   split index) to each 8 columns and writes global memory.
 #pragma once
 
 #include <cuda.h>
@@ -126,11 +126,18 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_tc_kernel(const __grid_cons
     if (ok) {
         const int row = m0 + warp * 32 + lane;
         const uint32_t lane_addr = tmem_d + (static_cast<uint32_t>(warp * 32) << 16);
+        static_assert(BN % 32 == 0, "the epilogue reads 32 accumulator columns at a time");
 #pragma unroll 1
-        for (int c = 0; c < BN; c += 8) {
-            float v[8];
-            tmem_ld8(lane_addr + static_cast<uint32_t>(c), v);
-            if (row < M && n0 + c < N) epi(static_cast<int>(blockIdx.z), row, n0 + c, v);
+        for (int c = 0; c < BN; c += 32) {
+            float v[32];
+            tmem_ld32(lane_addr + static_cast<uint32_t>(c), v);
+            if (row < M) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (n0 + c + 8 * q < N)
+                        epi(static_cast<int>(blockIdx.z), row, n0 + c + 8 * q,
+                            *reinterpret_cast<const float(*)[8]>(v + 8 * q));
+            }
         }
     }
     tc_fence_before();
