@@ -287,10 +287,11 @@ TMC_B200_API int tmc_b200_gemm_bf16(const uint16_t *A, const uint16_t *B, const 
  * captured in a CUDA graph. Matrices are row-major; "bf16" buffers are uint16_t bit patterns.
  * Every product runs on the tcgen05 tensor cores with FP32 accumulation (K multiple of 64).
  *
- * linear:        Z = X W^T + b (float32, optional), H = gelu(Z) or Z (bf16, optional);
- *                X: M x K, W: N x K, b: N.
- * backward_data: dX = (dZ WT^T) * gelu'(Zprev) (bf16); dZ: M x K, WT: N x K (the transposed
- *                weight, N = the layer's inputs), Zprev: M x N.
+ * linear:        Z = X W^T + b (float32, optional), H = gelu(Z) or Z (bf16, optional), HT = H^T
+ *                (bf16, N x M, optional: the operand of the weight gradient, written by the same
+ *                kernel); X: M x K, W: N x K, b: N.
+ * backward_data: dX = (dZ WT^T) * gelu'(Zprev) (bf16) and dXT = dX^T (N x M, optional); dZ: M x K,
+ *                WT: N x K (the transposed weight, N = the layer's inputs), Zprev: M x N.
  * matmul_f32:    D = A B^T (float32); A: M x K, B: N x K (weight gradients from transposed
  *                activations).
  * matmul_f32_splitk: the same with K cut into `splits` equal ranges computed by separate CTAs
@@ -310,9 +311,11 @@ TMC_B200_API int tmc_b200_gemm_bf16(const uint16_t *A, const uint16_t *B, const 
  * to_bf16:       wb = bf16(w) and wt = its transpose (each optional) for a rows x cols matrix.
  * status:        nonzero if a bounded tensor-core wait gave up since the last clear. */
 TMC_B200_API int tmc_b200_nn_linear(const uint16_t *X, const uint16_t *W, const float *bias, float *Z, uint16_t *H,
-                                    int32_t M, int32_t N, int32_t K, int32_t gelu, void *stream, tmc_status *status);
+                                    uint16_t *HT, int32_t M, int32_t N, int32_t K, int32_t gelu, void *stream,
+                                    tmc_status *status);
 TMC_B200_API int tmc_b200_nn_backward_data(const uint16_t *dZ, const uint16_t *WT, const float *Zprev, uint16_t *dX,
-                                           int32_t M, int32_t N, int32_t K, void *stream, tmc_status *status);
+                                           uint16_t *dXT, int32_t M, int32_t N, int32_t K, void *stream,
+                                           tmc_status *status);
 TMC_B200_API int tmc_b200_nn_matmul_f32(const uint16_t *A, const uint16_t *B, float *D, int32_t M, int32_t N,
                                         int32_t K, void *stream, tmc_status *status);
 TMC_B200_API int tmc_b200_nn_matmul_f32_splitk(const uint16_t *A, const uint16_t *B, float *D, float *work,

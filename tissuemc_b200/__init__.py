@@ -162,8 +162,8 @@ PROTOTYPES = {
     "tmc_b200_gemm_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
                                           _P(CStatus)]),
-    "tmc_b200_nn_linear": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.c_int32] * 4 + [ctypes.c_void_p, _P(CStatus)]),
-    "tmc_b200_nn_backward_data": (ctypes.c_int, [ctypes.c_void_p] * 4 + [ctypes.c_int32] * 3 +
+    "tmc_b200_nn_linear": (ctypes.c_int, [ctypes.c_void_p] * 6 + [ctypes.c_int32] * 4 + [ctypes.c_void_p, _P(CStatus)]),
+    "tmc_b200_nn_backward_data": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.c_int32] * 3 +
                                   [ctypes.c_void_p, _P(CStatus)]),
     "tmc_b200_nn_matmul_f32": (ctypes.c_int, [ctypes.c_void_p] * 3 + [ctypes.c_int32] * 3 + [ctypes.c_void_p, _P(CStatus)]),
     "tmc_b200_nn_matmul_f32_splitk": (ctypes.c_int, [ctypes.c_void_p] * 4 + [ctypes.c_int32] * 4 +

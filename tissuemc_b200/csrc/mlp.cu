@@ -71,12 +71,24 @@ struct EpiF32 {
     }
 };
 
-// Forward linear layer: z = acc + bias (stored as float32 if Z), h = act(z) (stored as bf16 if H).
+// h (bf16) also into HT, the transpose (N x M): lane = row, so a warp's stores of one column are
+// 32 consecutive bf16 (coalesced); this replaces a separate transpose pass.
+__device__ __forceinline__ void store_transposed(__nv_bfloat16 *HT, int M, int N, int row, int col,
+                                                 const float (&h)[8]) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        if (col + i < N) HT[static_cast<size_t>(col + i) * M + row] = __float2bfloat16_rn(h[i]);
+}
+
+// Forward linear layer: z = acc + bias (stored as float32 if Z), h = act(z) (stored as bf16 if H,
+// and transposed as bf16 if HT, an N x M matrix).
 struct EpiFwd {
     const float *bias;
     float *Z;
     __nv_bfloat16 *H;
     int N, act;
+    __nv_bfloat16 *HT;
+    int M;
     __device__ __forceinline__ void operator()(int, int row, int col, const float (&v)[8]) const {
         const size_t o = static_cast<size_t>(row) * N + col;
         float z[8], h[8];
@@ -85,6 +97,7 @@ struct EpiFwd {
             z[i] = v[i] + (col + i < N ? bias[col + i] : 0.0f);
             h[i] = act ? gelu(z[i]) : z[i];
         }
+        if (HT) store_transposed(HT, M, N, row, col, h);
         if (N % 8 == 0 && col + 8 <= N) {
             if (Z) {
                 reinterpret_cast<float4 *>(Z + o)[0] = make_float4(z[0], z[1], z[2], z[3]);
@@ -102,28 +115,32 @@ struct EpiFwd {
     }
 };
 
-// Backward through a linear layer into the previous GELU: dx = acc * gelu'(z_prev), bf16.
+// Backward through a linear layer into the previous GELU: dx = acc * gelu'(z_prev), bf16 (and
+// transposed into dXT, an N x M matrix, if given).
 struct EpiBwd {
     const float *Zprev;
     __nv_bfloat16 *dX;
     int N;
+    __nv_bfloat16 *dXT;
+    int M;
     __device__ __forceinline__ void operator()(int, int row, int col, const float (&v)[8]) const {
         const size_t o = static_cast<size_t>(row) * N + col;
+        float d[8];
         if (N % 8 == 0 && col + 8 <= N) {
             const float4 z0 = reinterpret_cast<const float4 *>(Zprev + o)[0];
             const float4 z1 = reinterpret_cast<const float4 *>(Zprev + o)[1];
             const float z[8] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
-            float d[8];
 #pragma unroll
             for (int i = 0; i < 8; ++i) d[i] = v[i] * gelu_grad(z[i]);
             *reinterpret_cast<uint4 *>(dX + o) = pack8_bf16(d);
         } else {
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                if (col + i >= N) break;
-                dX[o + i] = __float2bfloat16_rn(v[i] * gelu_grad(Zprev[o + i]));
+                d[i] = col + i < N ? v[i] * gelu_grad(Zprev[o + i]) : 0.0f;
+                if (col + i < N) dX[o + i] = __float2bfloat16_rn(d[i]);
             }
         }
+        if (dXT) store_transposed(dXT, M, N, row, col, d);
     }
 };
 
@@ -443,24 +460,29 @@ int tmc_b200_gemm_bf16(const uint16_t *A, const uint16_t *B, const float *bias, 
     return TMC_OK;
 }
 
-int tmc_b200_nn_linear(const uint16_t *X, const uint16_t *W, const float *bias, float *Z, uint16_t *H, int32_t M,
-                       int32_t N, int32_t K, int32_t gelu_act, void *stream, tmc_status *st) {
+int tmc_b200_nn_linear(const uint16_t *X, const uint16_t *W, const float *bias, float *Z, uint16_t *H, uint16_t *HT,
+                       int32_t M, int32_t N, int32_t K, int32_t gelu_act, void *stream, tmc_status *st) {
     put(st, TMC_OK, "");
-    if (!bias || (!Z && !H)) {
+    if (!bias || (!Z && !H && !HT)) {
         put(st, TMC_BAD_ARGUMENT, "NULL argument");
         return TMC_BAD_ARGUMENT;
     }
-    return launch_gemm(X, W, M, N, K, EpiFwd{bias, Z, reinterpret_cast<__nv_bfloat16 *>(H), N, gelu_act}, stream, st);
+    return launch_gemm(X, W, M, N, K,
+                       EpiFwd{bias, Z, reinterpret_cast<__nv_bfloat16 *>(H), N, gelu_act,
+                              reinterpret_cast<__nv_bfloat16 *>(HT), M},
+                       stream, st);
 }
 
-int tmc_b200_nn_backward_data(const uint16_t *dZ, const uint16_t *WT, const float *Zprev, uint16_t *dX, int32_t M,
-                              int32_t N, int32_t K, void *stream, tmc_status *st) {
+int tmc_b200_nn_backward_data(const uint16_t *dZ, const uint16_t *WT, const float *Zprev, uint16_t *dX, uint16_t *dXT,
+                              int32_t M, int32_t N, int32_t K, void *stream, tmc_status *st) {
     put(st, TMC_OK, "");
     if (!Zprev || !dX) {
         put(st, TMC_BAD_ARGUMENT, "NULL argument");
         return TMC_BAD_ARGUMENT;
     }
-    return launch_gemm(dZ, WT, M, N, K, EpiBwd{Zprev, reinterpret_cast<__nv_bfloat16 *>(dX), N}, stream, st);
+    return launch_gemm(dZ, WT, M, N, K,
+                       EpiBwd{Zprev, reinterpret_cast<__nv_bfloat16 *>(dX), N, reinterpret_cast<__nv_bfloat16 *>(dXT), M},
+                       stream, st);
 }
 
 int tmc_b200_nn_matmul_f32(const uint16_t *A, const uint16_t *B, float *D, int32_t M, int32_t N, int32_t K,

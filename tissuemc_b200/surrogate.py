@@ -166,38 +166,45 @@ class Member:
         self.work = torch.empty(self.splits * max(n * k for (k, n) in LAYER_DIMS), **f32)
         self.colsum_work = torch.empty(lib().tmc_b200_nn_colsum_work(max(n for (_, n) in LAYER_DIMS)), **f32)
         self.L = L
+        self._forward_for_training = False  # HT holds the transposed activations of the last forward pass
 
     def forward(self, X, rows: int, stream: int, Z_out=None):
-        """X: (rows, 64) bf16 -> the last layer's Z (rows, 128) float32 (into Z_out if given)."""
+        """X: (rows, 64) bf16 -> the last layer's Z (rows, 128) float32 (into Z_out if given). A
+        training forward pass (a full batch, Z_out not given) also writes the transposed
+        activations that backward() needs, from the same kernels."""
+        training = rows == self.B and Z_out is None
         h = X
         for li, (k, n) in enumerate(LAYER_DIMS):
             last = li == self.L - 1
             Z = (Z_out if (last and Z_out is not None) else self.Z[li])
             _call("tmc_b200_nn_linear", _p(h), _p(self.Wb[li]), _p(self.b[li]), _p(Z),
-                  _p(None if last else self.H[li]), rows, n, k, 0 if last else 1, ctypes.c_void_p(stream))
+                  _p(None if last else self.H[li]), _p(self.HT[li] if training and not last else None),
+                  rows, n, k, 0 if last else 1, ctypes.c_void_p(stream))
             if not last:
                 h = self.H[li]
+        self._forward_for_training = training
         return Z_out if Z_out is not None else self.Z[-1]
 
     def backward(self, X, Y, stream: int, scale: float):
-        """Loss and gradients for one full batch (X: B x 64 bf16, Y: B x 66 float32)."""
+        """Loss and gradients for one full batch (X: B x 64 bf16, Y: B x 66 float32), after the
+        training forward pass of the same batch."""
+        if not getattr(self, "_forward_for_training", False):
+            raise RuntimeError("backward() needs the training forward pass of the same batch first")
         B, s = self.B, ctypes.c_void_p(stream)
         self.loss.zero_()
         _call("tmc_b200_nn_mse", _p(self.Z[-1]), _p(Y), _p(self.dZ[-1]), _p(self.loss), B, N_OUT, N_OUT_PAD,
               ctypes.c_float(scale), s)
         _call("tmc_b200_nn_transpose", _p(X), _p(self.XT), B, K_IN, s)
-        for li in range(self.L - 1):
-            _call("tmc_b200_nn_transpose", _p(self.H[li]), _p(self.HT[li]), B, LAYER_DIMS[li][1], s)
+        _call("tmc_b200_nn_transpose", _p(self.dZ[-1]), _p(self.dZT[-1]), B, LAYER_DIMS[-1][1], s)
         for li in range(self.L - 1, -1, -1):
             k, n = LAYER_DIMS[li]
-            _call("tmc_b200_nn_transpose", _p(self.dZ[li]), _p(self.dZT[li]), B, n, s)
             prev_T = self.XT if li == 0 else self.HT[li - 1]
             _call("tmc_b200_nn_matmul_f32_splitk", _p(self.dZT[li]), _p(prev_T), _p(self.gW[li]), _p(self.work),
                   n, k, B, self.splits, s)
             _call("tmc_b200_nn_colsum", _p(self.dZ[li]), _p(self.gb[li]), B, n, _p(self.colsum_work), s)
-            if li > 0:
+            if li > 0:  # the gradient into the previous layer, and its transpose for that layer's product
                 _call("tmc_b200_nn_backward_data", _p(self.dZ[li]), _p(self.WT[li]), _p(self.Z[li - 1]),
-                      _p(self.dZ[li - 1]), B, k, n, s)
+                      _p(self.dZ[li - 1]), _p(self.dZT[li - 1]), B, k, n, s)
 
     def adam(self, stream: int, lr_t: float = 0.0, lr_dev=None, b1=0.9, b2=0.999, eps=1e-8, wd=0.0, avg=None,
              ema: float = 0.0):
