@@ -261,7 +261,7 @@ class Ensemble:
         the weights at the end.
 
         One optimiser step of the whole ensemble (batch gathers, forward, backward, Adam and
-        averaging: about 50 launches per member) runs once from the host and is then captured as a
+        averaging: 46 launches per member) runs once from the host and is then captured as a
         CUDA graph, one independent branch per member, that every later step replays; each step's
         batch indices and step size reach the graph through device buffers written before the
         replay. graph=False launches every kernel from the host, one member after the other. Both
