@@ -9,7 +9,7 @@ import subprocess
 import pytest
 
 import tissuemc_b200 as tmc
-from conftest import ROOT, has_gpu
+from conftest import has_gpu
 
 CLI = str(tmc.CLI_PATH)
 SLAB = str(tmc.CONFIGS / "slab_n14.mci")
