@@ -10,8 +10,8 @@
 // the BatchPlan batches with the right sizes.
 //
 // Sweep (sweep_kernel.cuh, sweep.cu): the item queue covers every photon of every configuration
-// exactly once for ragged photon counts and item sizes, and the item order's stride is coprime
-// with the item count.
+// exactly once for ragged photon counts, item sizes and band counts; each band's order is a
+// permutation of that band, taken before the next band; the strides are coprime with the counts.
 
 #include <cstdint>
 #include <cstdio>
@@ -118,7 +118,7 @@ void walk_case(uint32_t N, int W, uint32_t chunk, uint32_t nb, uint64_t seed) {
                static_cast<unsigned long long>(per_batch[b]));
 }
 
-void sweep_case(const std::vector<uint32_t> &photons, uint32_t item) {
+void sweep_case(const std::vector<uint32_t> &photons, uint32_t item, uint32_t bands) {
     const uint32_t n_cfg = static_cast<uint32_t>(photons.size());
     std::vector<uint32_t> prefix(n_cfg + 1u, 0u);
     uint64_t total = 0;
@@ -127,13 +127,16 @@ void sweep_case(const std::vector<uint32_t> &photons, uint32_t item) {
         total += (photons[c] + item - 1u) / item;
     }
     prefix[n_cfg] = static_cast<uint32_t>(total);
-    const uint32_t perm = tmc::sweep_perm(total);
+    const tmc::SweepOrder order = tmc::sweep_order(static_cast<uint32_t>(total), bands);
     std::vector<std::vector<uint8_t>> covered(n_cfg);
     for (uint32_t c = 0; c < n_cfg; ++c) covered[c].assign(photons[c], 0);
     for (uint32_t idx = 0; idx < total; ++idx) {
+        const uint32_t j = order.item(idx);  // inside the band of idx: bands are taken in order
+        EXPECT(j / order.band == idx / order.band, "item %u of band %u lands in band %u", idx, idx / order.band,
+               j / order.band);
         uint32_t cfg = 0, first = 0, end = 0;
-        tmc::sweep_item(idx, static_cast<uint32_t>(total), perm, item, n_cfg, prefix.data(),
-                        [&](uint32_t c) { return photons[c]; }, cfg, first, end);
+        tmc::sweep_item(idx, order, item, n_cfg, prefix.data(), [&](uint32_t c) { return photons[c]; }, cfg, first,
+                        end);
         EXPECT(cfg < n_cfg && first < end && end <= photons[cfg] && end - first <= item,
                "item %u -> cfg %u [%u, %u)", idx, cfg, first, end);
         for (uint32_t p = first; p < end; ++p) {
@@ -169,18 +172,39 @@ int main() {
     for (const auto &c : walks)
         for (int rep = 0; rep < 3; ++rep) walk_case(c.N, c.W, c.chunk, c.nb, seed++);
 
-    // sweep: single photons, item-size edges, ragged random counts, thousands of configurations
-    sweep_case({1}, 256);
-    sweep_case({255, 256, 257, 512, 1}, 256);
-    std::mt19937_64 rng(7);
-    for (uint32_t item : {1u, 7u, 64u, 256u, 1024u}) {
-        std::vector<uint32_t> ph(1 + rng() % 300);
-        for (uint32_t &p : ph) p = 1 + static_cast<uint32_t>(rng() % 5000);
-        sweep_case(ph, item);
+    // sweep: single photons, item-size edges, ragged random counts, thousands of configurations,
+    // one band to more bands than items
+    for (uint32_t bands : {1u, 3u, 16u, 1000u}) {
+        sweep_case({1}, 256, bands);
+        sweep_case({255, 256, 257, 512, 1}, 256, bands);
+        std::mt19937_64 rng(7 + bands);
+        for (uint32_t item : {1u, 7u, 64u, 256u, 1024u}) {
+            std::vector<uint32_t> ph(1 + rng() % 300);
+            for (uint32_t &p : ph) p = 1 + static_cast<uint32_t>(rng() % 5000);
+            sweep_case(ph, item, bands);
+        }
+        std::vector<uint32_t> many(4096);
+        for (uint32_t &p : many) p = 1 + static_cast<uint32_t>(rng() % 3000);
+        sweep_case(many, 256, bands);
     }
-    std::vector<uint32_t> many(4096);
-    for (uint32_t &p : many) p = 1 + static_cast<uint32_t>(rng() % 3000);
-    sweep_case(many, 256);
+
+    // every band's order is a permutation of the band, for item counts and band counts around
+    // the edges (a last band shorter than the others, bands of one item)
+    for (uint32_t total = 1; total < 3000; ++total)
+        for (uint32_t bands : {1u, 2u, 7u, 16u}) {
+            const tmc::SweepOrder order = tmc::sweep_order(total, bands);
+            std::vector<uint8_t> seen(total, 0);
+            for (uint32_t idx = 0; idx < total; ++idx) {
+                const uint32_t j = order.item(idx);
+                if (j >= total || seen[j]) {
+                    std::fprintf(stderr, "FAILED: %u items in %u bands: item %u taken twice or out of range\n",
+                                 total, bands, j);
+                    ++g_failures;
+                    return 1;
+                }
+                seen[j] = 1;
+            }
+        }
 
     // the item order's stride is coprime with every item count (so the order is a permutation)
     for (uint64_t total = 0; total < 200000; ++total) {

@@ -6,9 +6,11 @@
 // same seed, photons, batches and grid.
 //
 // Work is a queue of items (configuration, first photon, count): configuration c's photons in
-// chunks of item_photons, numbered through a prefix sum and taken in a strided permutation of
-// that numbering, so that the warps at work at any moment are spread over many configurations
-// (their tallies then rarely meet on one L2 line). A warp takes items one at a time and hands their
+// chunks of item_photons, numbered through a prefix sum and taken band by band, in a strided
+// permutation inside each band (work_queue.cuh, SweepOrder), so that the warps at work at any
+// moment are spread over many configurations (their tallies then rarely meet on one L2 line). The
+// host lays the configurations out longest photons first, so the bands run from the configurations
+// whose photons take the most steps to those whose photons take the fewest. A warp takes items one at a time and hands their
 // photons to its idle lanes; every lane carries the
 // configuration of its own photon (Philox key, layer table pointer, tally base), so a warp moves
 // on to the next item while some of its lanes still finish photons of the previous one, and no
@@ -37,9 +39,9 @@ static_assert(sizeof(SweepConfigC) == 48, "SweepConfigC layout");
 // captured graph serves sweeps of different sizes).
 struct SweepHeader {
     uint32_t n_cfg;         // configurations
-    uint32_t total_items;   // work items: configuration c has ceil(photons_c / item_photons)
-    uint32_t perm;          // items are taken in the order j = i * perm mod total_items
     uint32_t item_photons;  // photons per item (the last item of a configuration may hold fewer)
+    SweepOrder order;       // order.total items (configuration c has ceil(photons_c / item_photons))
+                            // and the order in which they are taken
 };
 
 struct SweepParams {
@@ -137,7 +139,7 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                      0ull};
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const SweepHeader H = *P.hdr;
+    const SweepHeader &H = *P.hdr;  // read where an item is taken (rare), not held in registers
 
     // warp-uniform: the item being handed out
     uint32_t it_cfg = 0u, it_next = 0u, it_end = 0u;
@@ -156,8 +158,8 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                     uint32_t idx = 0u;
                     if (static_cast<int>(lane) == leader) idx = atomicAdd(P.item_counter, 1u);
                     idx = __shfl_sync(0xffffffffu, idx, leader);
-                    if (idx < H.total_items) {
-                        sweep_item(idx, H.total_items, H.perm, H.item_photons, H.n_cfg, P.prefix,
+                    if (idx < H.order.total) {
+                        sweep_item(idx, H.order, H.item_photons, H.n_cfg, P.prefix,
                                    [&](uint32_t c) { return P.cfgs[c].photons; }, it_cfg, it_next, it_end);
                         continue;
                     }

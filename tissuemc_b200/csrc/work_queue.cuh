@@ -1,5 +1,6 @@
 // How the persistent kernels hand out work: the photon-id pool of a warp (walk_kernel.cuh), the
-// batch of a photon id, and the item queue of the batched sweep (sweep_kernel.cuh, sweep.cu).
+// batch of a photon id, and the item queue of the batched sweep and its order (sweep_kernel.cuh,
+// sweep.cu).
 //
 // The code has no CUDA intrinsics, so it compiles for the host as well: the warp-level choices
 // (who claims, which lane gets which id) are made by the callers with ballots and shuffles, and
@@ -52,16 +53,32 @@ struct WarpPool {
     }
 };
 
-// Item `idx` of the sweep's queue (0 <= idx < total). Configuration c owns items prefix[c] ..
-// prefix[c + 1] - 1, each of item_photons photons (its last one fewer when photons_of(c) is not a
-// multiple); items are taken in the order j = idx * perm mod total (perm coprime with total, so
-// this is a permutation), which spreads the warps at work over many configurations. Gives the
-// configuration, its first photon and one past its last.
+// The order in which the sweep's items are taken: the item range is cut into bands of `band`
+// items (the last one may be shorter), taken one band after the other; inside a band, item idx
+// maps to start + (idx - start) * p mod size with p coprime with the band's size (perm, or
+// perm_last for a shorter last band), which spreads the warps at work over many configurations.
+// The host lays configurations out so that the first bands hold the longest photons: those start
+// early, and the launch does not end waiting for one long photon that started last.
+struct SweepOrder {
+    uint32_t total, band, perm, perm_last;
+
+    TMC_HD uint32_t item(uint32_t idx) const {
+        const uint32_t start = idx / band * band;
+        const uint32_t size = total - start < band ? total - start : band;
+        const uint32_t p = size == band ? perm : perm_last;
+        return start + static_cast<uint32_t>((static_cast<uint64_t>(idx - start) * p) % size);
+    }
+};
+
+// Item `idx` of the sweep's queue (0 <= idx < order.total), taken as order.item(idx).
+// Configuration c owns items prefix[c] .. prefix[c + 1] - 1, each of item_photons photons (its last
+// one fewer when photons_of(c) is not a multiple). Gives the configuration, its first photon and
+// one past its last.
 template <class PhotonsOf>
-TMC_HD void sweep_item(uint32_t idx, uint32_t total, uint32_t perm, uint32_t item_photons, uint32_t n_cfg,
+TMC_HD void sweep_item(uint32_t idx, const SweepOrder &order, uint32_t item_photons, uint32_t n_cfg,
                        const uint32_t *prefix, PhotonsOf photons_of, uint32_t &cfg, uint32_t &first,
                        uint32_t &end) {
-    const uint32_t j = static_cast<uint32_t>((static_cast<uint64_t>(idx) * perm) % total);
+    const uint32_t j = order.item(idx);
     uint32_t lo = 0u, hi = n_cfg;  // the c with prefix[c] <= j < prefix[c + 1]
     while (hi - lo > 1u) {
         const uint32_t mid = (lo + hi) >> 1;
@@ -74,7 +91,7 @@ TMC_HD void sweep_item(uint32_t idx, uint32_t total, uint32_t perm, uint32_t ite
     end = first + (left < item_photons ? left : item_photons);
 }
 
-// The stride of the sweep's item order: the first of a few large odd multipliers whose residue is
+// A stride for a band of `total` items: the first of a few large odd multipliers whose residue is
 // coprime with `total` (1, the plain order, when none is or total < 2).
 inline uint32_t sweep_perm(uint64_t total) {
     constexpr uint32_t kCandidates[] = {2654435761u, 2246822519u, 3266489917u, 668265263u, 374761393u};
@@ -89,6 +106,14 @@ inline uint32_t sweep_perm(uint64_t total) {
         if (a == 1) return static_cast<uint32_t>(p % total);
     }
     return 1u;
+}
+
+// The order for `total` items (total >= 1) in at most `bands` bands.
+inline SweepOrder sweep_order(uint32_t total, uint32_t bands) {
+    const uint32_t nb = bands < 1u ? 1u : (bands < total ? bands : total);
+    const uint32_t band = (total + nb - 1u) / nb;
+    const uint32_t last = total - (total - 1u) / band * band;
+    return SweepOrder{total, band, sweep_perm(band), sweep_perm(last)};
 }
 
 }  // namespace tmc
