@@ -10,13 +10,14 @@
 // permutation inside each band (work_queue.cuh, SweepOrder), so that the warps at work at any
 // moment are spread over many configurations (their tallies then rarely meet on one L2 line). The
 // host lays the configurations out longest photons first, so the bands run from the configurations
-// whose photons take the most steps to those whose photons take the fewest. A warp takes items one at a time and hands their
-// photons to its idle lanes; every lane carries the
-// configuration of its own photon (Philox key, layer table pointer, tally base), so a warp moves
-// on to the next item while some of its lanes still finish photons of the previous one, and no
-// lane waits for an item to drain. Tallies of configuration c live at tally + c * stride in the
-// single-run layout (batch totals, A(r,z), R_d(r,a), T_t(r,a)), accumulated with 64-bit integer
-// atomics in global memory (L2); a per-lane run cache merges consecutive deposits into one bin.
+// whose photons take the most steps to those whose photons take the fewest. A warp takes items one
+// at a time and hands their photons to its idle lanes; every lane carries the configuration of its
+// own photon (its Philox key schedule in shared memory, written when the lane changes
+// configuration; the layer table pointer; the tally base), so a warp moves on to the next item
+// while some of its lanes still finish photons of the previous one, and no lane waits for an item
+// to drain. Tallies of configuration c live at tally + c * stride in the single-run layout (batch
+// totals, A(r,z), R_d(r,a), T_t(r,a)), accumulated with 64-bit integer atomics in global memory
+// (L2); a per-lane run cache merges consecutive deposits into one bin.
 #pragma once
 
 #include "walk_step.cuh"
@@ -64,8 +65,9 @@ template <int FAST> struct SweepCtx {
     Ring ring;
     uint32_t step_cap;
     int a_off, rd_off, tt_off, bstride;  // word offsets inside one configuration's tallies
-    // the configuration of this lane's current photon
-    uint32_t k0, k1;
+    // the configuration of this lane's current photon, and its Philox key schedule (shared memory)
+    uint32_t cfg;
+    uint4 *sched;
     int nl;
     const LayerC *layers;
     unsigned long long *t;
@@ -73,7 +75,7 @@ template <int FAST> struct SweepCtx {
     int cache_key;
     unsigned long long cache_val;
 
-    __device__ __forceinline__ void refill(Lane &L) const { ring.refill(L, k0, k1); }
+    __device__ __forceinline__ void refill(Lane &L) const { ring.refill(L, sched, static_cast<int>(P.threads)); }
     __device__ __forceinline__ uint32_t draw(Lane &L) const { return ring.draw(L); }
     __device__ __forceinline__ const LayerC &layer(const Lane &, int l) const { return layers[l]; }
     __device__ __forceinline__ int num_layers(const Lane &) const { return nl; }
@@ -130,8 +132,9 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                      P.nb * (4 + P.lmax) + P.nr * P.nz,
                      P.nb * (4 + P.lmax) + P.nr * P.nz + P.nr * P.na,
                      4 + P.lmax,
-                     0u,
-                     0u,
+                     0xFFFFFFFFu,
+                     // after the rings (8 words per lane): 5 x 16 bytes of key schedule per lane
+                     reinterpret_cast<uint4 *>(reinterpret_cast<uint32_t *>(smem) + 8 * P.threads) + threadIdx.x,
                      1,
                      P.layers,
                      P.tally,
@@ -175,8 +178,10 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
             if (mine) {
                 const SweepConfigC cf = P.cfgs[it_cfg];
                 const uint32_t id = it_next + rank;
-                C.k0 = cf.k0;
-                C.k1 = cf.k1;
+                if (it_cfg != C.cfg) {  // the lane's key schedule follows its configuration
+                    C.cfg = it_cfg;
+                    key_schedule_store(C.sched, static_cast<int>(P.threads), cf.k0, cf.k1);
+                }
                 C.nl = cf.nl;
                 C.layers = P.layers + cf.layer_base;
                 C.t = P.tally + static_cast<size_t>(it_cfg) * static_cast<size_t>(P.stride);

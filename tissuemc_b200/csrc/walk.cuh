@@ -116,6 +116,45 @@ __device__ __forceinline__ void philox4x32_10_rk(uint32_t c0, uint32_t c1, uint3
     o3 = c3;
 }
 
+// The key schedule of `key` (k0, k1 of rounds 0..9: k + r * (0x9E3779B9, 0xBB67AE85)) stored for
+// one lane as five 16-byte words in shared memory, sched[q * stride] = rounds 2q and 2q + 1; a
+// warp's load of word q reads 32 consecutive 16-byte words (no bank conflict).
+__device__ __forceinline__ void key_schedule_store(uint4 *sched, int stride, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        sched[q * stride] = make_uint4(k0, k1, k0 + 0x9E3779B9u, k1 + 0xBB67AE85u);
+        k0 += 2u * 0x9E3779B9u;
+        k1 += 2u * 0xBB67AE85u;
+    }
+}
+
+// The same rounds with the key schedule read from shared memory (key_schedule_store): for lanes
+// whose keys differ, where a schedule in the parameter bank cannot serve them all.
+__device__ __forceinline__ void philox4x32_10_sched(uint32_t c0, uint32_t c1, uint32_t c2, const uint4 *sched,
+                                                    int stride, uint32_t &o0, uint32_t &o1, uint32_t &o2,
+                                                    uint32_t &o3) {
+    uint32_t c3 = 0u;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        const uint4 k = sched[q * stride];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * c0;
+            const uint64_t p1 = static_cast<uint64_t>(0xCD9E8D57u) * c2;
+            const uint32_t n0 = static_cast<uint32_t>(p1 >> 32) ^ c1 ^ (h ? k.z : k.x);
+            const uint32_t n2 = static_cast<uint32_t>(p0 >> 32) ^ c3 ^ (h ? k.w : k.y);
+            c0 = n0;
+            c1 = static_cast<uint32_t>(p1);
+            c2 = n2;
+            c3 = static_cast<uint32_t>(p0);
+        }
+    }
+    o0 = c0;
+    o1 = c1;
+    o2 = c2;
+    o3 = c3;
+}
+
 // Uniform on (0,1) from one word, keeping 23 bits (philox.hpp:133-136).
 // The value is ((x >> 9) + 1/2) * 2^-23, computed without an integer-to-float conversion: the 23
 // kept bits become the mantissa of a float in [1, 2), 1 + m 2^-23, and subtracting 1 - 2^-24 gives

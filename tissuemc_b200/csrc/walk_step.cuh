@@ -318,6 +318,12 @@ struct Ring {
         philox4x32_10_rk(L.id, 0u, L.blk, rk, b0, b1, b2, b3);
         store(L, b0, b1, b2, b3);
     }
+    // with this lane's key schedule in shared memory (key_schedule_store)
+    __device__ __forceinline__ void refill(Lane &L, const uint4 *sched, int sched_stride) const {
+        uint32_t b0, b1, b2, b3;
+        philox4x32_10_sched(L.id, 0u, L.blk, sched, sched_stride, b0, b1, b2, b3);
+        store(L, b0, b1, b2, b3);
+    }
 };
 
 }  // namespace tmc
