@@ -70,7 +70,7 @@ template <int FAST> struct SweepCtx {
     uint4 *sched;
     int nl;
     const LayerC *layers;
-    unsigned long long *t;
+    int t;  // word offset of the configuration's tallies in P.tally (they hold < 2^31 words)
     // run cache: word index into P.tally of the last A(r,z) bin, and its pending value
     int cache_key;
     unsigned long long cache_val;
@@ -80,14 +80,14 @@ template <int FAST> struct SweepCtx {
     __device__ __forceinline__ const LayerC &layer(const Lane &, int l) const { return layers[l]; }
     __device__ __forceinline__ int num_layers(const Lane &) const { return nl; }
     __device__ __forceinline__ void batch_add(const Lane &L, int slot, unsigned long long v) const {
-        atomicAdd(&t[L.batch * bstride + slot], v);
+        atomicAdd(&P.tally[t + L.batch * bstride + slot], v);
     }
     __device__ __forceinline__ void absorb(const Lane &L, unsigned long long v) {
         if (!P.profiles) return;
         const float rr = radius<FAST>(L.x, L.y);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int iz = bin_of<FAST>(L.z, P.dz, P.inv_dz, P.nz);
-        const int key = static_cast<int>(t - P.tally) + a_off + ir * P.nz + iz;
+        const int key = t + a_off + ir * P.nz + iz;
         if (key == cache_key) {
             cache_val += v;
         } else {
@@ -105,7 +105,7 @@ template <int FAST> struct SweepCtx {
         const float rr = radius<FAST>(L.x, L.y);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int ia = P.na > 1 ? bin_of<FAST>(acosf(fminf(fabsf(L.uz), 1.0f)), P.da, P.inv_da, P.na) : 0;
-        atomicAdd(&t[(kind == 1 ? rd_off : tt_off) + ir * P.na + ia], v);
+        atomicAdd(&P.tally[t + (kind == 1 ? rd_off : tt_off) + ir * P.na + ia], v);
     }
 };
 
@@ -137,7 +137,7 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                      reinterpret_cast<uint4 *>(reinterpret_cast<uint32_t *>(smem) + 8 * P.threads) + threadIdx.x,
                      1,
                      P.layers,
-                     P.tally,
+                     0,
                      -1,
                      0ull};
     const unsigned lane = threadIdx.x & 31u;
@@ -184,7 +184,7 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                 }
                 C.nl = cf.nl;
                 C.layers = P.layers + cf.layer_base;
-                C.t = P.tally + static_cast<size_t>(it_cfg) * static_cast<size_t>(P.stride);
+                C.t = static_cast<int>(it_cfg) * P.stride;
                 const int batch = batch_of(id, cf.plan_base, cf.plan_extra, cf.plan_bnd);
                 launch(L, C, id, batch, cf.launch_w);
                 alive = true;
