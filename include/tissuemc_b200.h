@@ -254,10 +254,16 @@ TMC_B200_API int tmc_b200_sweep_sample(uint64_t master_seed, int32_t n, tmc_swee
 TMC_B200_API int tmc_b200_sweep_sizes(const tmc_sweep_config *cfgs, int32_t n, const tmc_sweep_options *opt,
                                       tmc_sweep_sizes *sizes, tmc_status *status);
 
+/* The estimate of the steps a photon of each configuration takes, by which tmc_b200_sweep_run
+ * orders the configurations inside its launch (largest first, so that long photons start early);
+ * host only, for inspection. cost: n doubles. */
+TMC_B200_API int tmc_b200_sweep_costs(const tmc_sweep_config *cfgs, int32_t n, double *cost, tmc_status *status);
+
 /* Run the sweep: one captured graph (table upload, zeroing, the persistent sweep kernel, the
  * per-configuration summary kernel, summary download), cached per device and reused while the
  * shape allows. raw (optional, host): n * words_per_config words; summary (optional, host):
- * n * summary_per_config doubles; kernel_seconds (optional): device time of the sweep kernel. */
+ * n * summary_per_config doubles, both in the order of cfgs; kernel_seconds (optional): device
+ * time of the sweep kernel. */
 TMC_B200_API int tmc_b200_sweep_run(const tmc_sweep_config *cfgs, int32_t n, const tmc_sweep_options *opt,
                                     uint64_t *raw, double *summary, double *kernel_seconds, tmc_status *status);
 

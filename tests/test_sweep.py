@@ -1,4 +1,5 @@
-"""The batched sweep: the configuration sampler and validation (CPU), and on the GPU bit-for-bit
+"""The batched sweep: the configuration sampler, validation and the photon-cost estimate that orders
+configurations inside a launch (CPU, the estimate against the oracle), and on the GPU bit-for-bit
 agreement of every configuration with its own single run, graph reuse across sweeps, the plain
 loop baseline, the autotuner, the per-configuration summaries, and oracle parity on a few
 configurations."""
@@ -66,6 +67,33 @@ def _single_run_raw(c, opt):
     spec = tmc.config_spec(c, opt)
     r = tmc.run(spec, photons=int(c.photons), batches=opt.batches, seed=int(c.seed), fast_math=bool(opt.fast_math))
     return r
+
+
+def test_photon_cost_estimate_ranks_configurations_like_the_oracle():
+    """The sweep runs its configurations longest photons first by an estimate of the steps per
+    photon; its ranking agrees with the steps the float64 oracle measures (one photon per batch)."""
+    from scipy.stats import spearmanr
+
+    cfgs = tmc.sweep_sample(1, 256)
+    cost = tmc.sweep_costs(cfgs)
+    assert np.isfinite(cost).all() and (cost > 0).all()
+    opt = tmc.sweep_options()
+    measured = []
+    for c in cfgs:
+        spec = tmc.config_spec(c, opt)
+        o = oracle.run(oracle.Spec(layers=list(spec.layers), dz=spec.dz, dr=spec.dr, nz=1, nr=1, na=1,
+                                   n_above=spec.n_above, n_below=spec.n_below), 64, 64, int(c.seed), 64)
+        measured.append(float((o.events + o.boundary_steps).mean()))
+    rho = spearmanr(cost, measured).correlation
+    assert rho > 0.9, rho
+    # the heaviest quarter by the estimate holds most of the heaviest quarter by measurement
+    k = len(cfgs) // 4
+    top_est, top_meas = set(np.argsort(-cost)[:k]), set(np.argsort(-np.array(measured))[:k])
+    assert len(top_est & top_meas) >= 0.75 * k
+    with pytest.raises(tmc.ConfigError, match="configuration 1"):
+        bad = tmc.sweep_sample(1, 2)
+        bad[1].num_layers = 0
+        tmc.sweep_costs(bad)
 
 
 @pytest.mark.gpu

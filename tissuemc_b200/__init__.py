@@ -151,6 +151,7 @@ PROTOTYPES = {
     "tmc_b200_write_mco": (ctypes.c_int, [_P(CRunSpec), _P(COptions), _P(CResult), ctypes.c_char_p, _P(CStatus)]),
     "tmc_b200_sweep_default_options": (None, [_P(CSweepOptions)]),
     "tmc_b200_sweep_sample": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int32, _P(CSweepConfig), _P(CStatus)]),
+    "tmc_b200_sweep_costs": (ctypes.c_int, [_P(CSweepConfig), ctypes.c_int32, _P(ctypes.c_double), _P(CStatus)]),
     "tmc_b200_sweep_sizes": (ctypes.c_int, [_P(CSweepConfig), ctypes.c_int32, _P(CSweepOptions),
                                             _P(CSweepSizes), _P(CStatus)]),
     "tmc_b200_sweep_run": (ctypes.c_int, [_P(CSweepConfig), ctypes.c_int32, _P(CSweepOptions), _pu, _pd, _pd,
@@ -552,6 +553,17 @@ def sweep_sample(master_seed: int, n: int):
     st = CStatus()
     _check(lib().tmc_b200_sweep_sample(master_seed, n, arr, ctypes.byref(st)), st)
     return arr
+
+
+
+def sweep_costs(cfgs) -> np.ndarray:
+    """The estimated steps per photon of each configuration, by which a sweep orders them inside
+    its launch (largest first)."""
+    arr = cfgs if isinstance(cfgs, ctypes.Array) else (CSweepConfig * len(cfgs))(*cfgs)
+    out = np.zeros(len(arr), dtype=np.float64)
+    st = CStatus()
+    _check(lib().tmc_b200_sweep_costs(arr, len(arr), out.ctypes.data_as(_P(ctypes.c_double)), ctypes.byref(st)), st)
+    return out
 
 
 def sweep_config(spec: RunSpec, photons: int, seed: int) -> CSweepConfig:

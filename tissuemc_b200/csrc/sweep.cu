@@ -434,6 +434,22 @@ int tmc_b200_sweep_sample(uint64_t master_seed, int32_t n, tmc_sweep_config *out
     return TMC_OK;
 }
 
+int tmc_b200_sweep_costs(const tmc_sweep_config *cfgs, int32_t n, double *cost, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!cfgs || !cost || n < 0) {
+        put(st, TMC_BAD_ARGUMENT, "NULL argument or negative count");
+        return TMC_BAD_ARGUMENT;
+    }
+    for (int c = 0; c < n; ++c) {
+        if (cfgs[c].num_layers < 1 || cfgs[c].num_layers > TMC_B200_MAX_LAYERS) {
+            put(st, TMC_BAD_CONFIG, "configuration " + std::to_string(c) + ": 1 to 16 layers are needed");
+            return TMC_BAD_CONFIG;
+        }
+        cost[c] = photon_cost(cfgs[c]);
+    }
+    return TMC_OK;
+}
+
 int tmc_b200_sweep_sizes(const tmc_sweep_config *cfgs, int32_t n, const tmc_sweep_options *opt,
                          tmc_sweep_sizes *sz, tmc_status *st) {
     put(st, TMC_OK, "");
