@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -175,37 +176,48 @@ __global__ void colsum_partial_kernel(const __nv_bfloat16 *__restrict__ dZ, floa
     part[static_cast<size_t>(blockIdx.y) * N + n] = (s[0] + s[1]) + (s[2] + s[3]);
 }
 
+// One warp per column: lane l adds partial rows l, l + 32, ... in order, then a fixed shuffle tree
+// adds the lanes (deterministic, and 32 loads in flight per column instead of one).
 __global__ void colsum_final_kernel(const float *__restrict__ part, float *__restrict__ db, int N, int groups) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N) return;
-    float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    int y = 0;
-    for (; y + 3 < groups; y += 4) {
+    const int n = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (n >= N) return;  // warp-uniform
+    float acc = 0.0f;
+    for (int y = lane; y < groups; y += 32) acc += part[static_cast<size_t>(y) * N + n];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) s[u] += part[static_cast<size_t>(y + u) * N + n];
-    }
-    for (; y < groups; ++y) s[0] += part[static_cast<size_t>(y) * N + n];
-    db[n] = (s[0] + s[1]) + (s[2] + s[3]);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) db[n] = acc;
 }
 
 // Mean-squared error over the first T of ld columns: loss += scale * sum (p - t)^2 and
-// dZ = 2 * scale * (p - t) (bf16; zero in the padded columns).
+// dZ = 2 * scale * (p - t) (bf16; zero in the padded columns). Grid-stride over the elements; each
+// block adds its partial loss once (one atomic per block rather than per warp).
 __global__ void mse_kernel(const float *__restrict__ pred, const float *__restrict__ target, __nv_bfloat16 *dZ,
                            float *loss, int M, int T, int ld, float scale) {
-    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    __shared__ float warp_sum[32];
+    const size_t n = static_cast<size_t>(M) * ld;
     float l = 0.0f;
-    if (i < static_cast<size_t>(M) * ld) {
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
         const int row = static_cast<int>(i / ld), col = static_cast<int>(i % ld);
         float g = 0.0f;
         if (col < T) {
             const float d = pred[i] - target[static_cast<size_t>(row) * T + col];
-            l = d * d;
+            l += d * d;
             g = 2.0f * scale * d;
         }
         if (dZ) dZ[i] = __float2bfloat16_rn(g);
     }
-    for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
-    if ((threadIdx.x & 31) == 0 && l != 0.0f) atomicAdd(loss, l * scale);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        l = threadIdx.x < (blockDim.x >> 5) ? warp_sum[threadIdx.x] : 0.0f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+        if (threadIdx.x == 0 && l != 0.0f) atomicAdd(loss, l * scale);
+    }
 }
 
 // Polyak averaging of one value: avg = beta avg + (1 - beta) w, with its rounding pinned so that
@@ -534,7 +546,7 @@ int tmc_b200_nn_colsum(const uint16_t *dZ, float *db, int32_t M, int32_t N, floa
     const int groups = M < kColsumGroups ? M : kColsumGroups;
     colsum_partial_kernel<<<dim3((N + 127) / 128, groups), 128, 0, s>>>(reinterpret_cast<const __nv_bfloat16 *>(dZ),
                                                                       work, M, N);
-    colsum_final_kernel<<<(N + 127) / 128, 128, 0, s>>>(work, db, N, groups);
+    colsum_final_kernel<<<(N + 7) / 8, 256, 0, s>>>(work, db, N, groups);  // 8 columns (warps) per block
     return launched(st);
 }
 
@@ -548,7 +560,8 @@ int tmc_b200_nn_mse(const float *pred, const float *target, uint16_t *dZ, float 
         return TMC_BAD_ARGUMENT;
     }
     const size_t n = static_cast<size_t>(M) * ld;
-    mse_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+    const size_t blocks = std::min<size_t>((n + 255) / 256, 1184);  // at most 8 blocks per SM of a B200
+    mse_kernel<<<static_cast<unsigned>(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         pred, target, reinterpret_cast<__nv_bfloat16 *>(dZ), loss, M, T, ld, scale);
     return launched(st);
 }
