@@ -313,6 +313,12 @@ TMC_B200_API int tmc_b200_gemm_bf16(const uint16_t *A, const uint16_t *B, const 
  *                when lr_dev (device memory) is given, so that a captured CUDA graph reads each
  *                step's value; with avg given, avg = avg_beta avg + (1 - avg_beta) w afterwards
  *                (Polyak averaging fused into the step, the same bits as the separate ema).
+ * adam_plan:     fill first_block of each tmc_adam_tensor of a host table (in order) and return
+ *                the blocks a launch over all of them needs (-1 on an empty or invalid table).
+ * adam_multi:    the adam step for every tensor of a planned table in one launch; `tab` is the
+ *                table copied to device memory, `blocks` what adam_plan returned; each tensor's
+ *                optional pointers (wb, wt, avg) may be NULL. The same bits as one adam call per
+ *                tensor.
  * ema:           avg = beta avg + (1 - beta) w over n float32 values (Polyak averaging).
  * to_bf16:       wb = bf16(w) and wt = its transpose (each optional) for a rows x cols matrix.
  * status:        nonzero if a bounded tensor-core wait gave up since the last clear. */
@@ -338,6 +344,23 @@ TMC_B200_API int tmc_b200_nn_adam(float *w, const float *g, float *m, float *v, 
                                   float lr_t, const float *lr_dev, float b1, float b2, float eps, float weight_decay,
                                   uint16_t *wb, uint16_t *wt, float *avg, float avg_beta, void *stream,
                                   tmc_status *status);
+/* One parameter tensor of a many-tensor Adam step (device pointers; rows x cols float32). */
+typedef struct {
+    float *w;
+    const float *g;
+    float *m;
+    float *v;
+    uint16_t *wb;  /* bf16 copy (optional) */
+    uint16_t *wt;  /* its transpose (optional) */
+    float *avg;    /* Polyak average (optional) */
+    int32_t rows, cols;
+    float weight_decay;
+    int32_t first_block; /* filled by tmc_b200_nn_adam_plan */
+} tmc_adam_tensor;
+TMC_B200_API int32_t tmc_b200_nn_adam_plan(tmc_adam_tensor *tab, int32_t count);
+TMC_B200_API int tmc_b200_nn_adam_multi(const tmc_adam_tensor *tab, int32_t count, int32_t blocks, float lr_t,
+                                        const float *lr_dev, float b1, float b2, float eps, float avg_beta,
+                                        void *stream, tmc_status *status);
 TMC_B200_API int tmc_b200_nn_ema(const float *w, float *avg, int64_t n, float beta, void *stream, tmc_status *status);
 TMC_B200_API int tmc_b200_nn_to_bf16(const float *w, int32_t rows, int32_t cols, uint16_t *wb, uint16_t *wt,
                                      void *stream, tmc_status *status);

@@ -45,6 +45,7 @@ def test_struct_sizes_match_the_header_layout():
     assert ctypes.sizeof(tmc.Layer) == 40
     assert ctypes.sizeof(tmc.CRunSpec) == 8 + 16 + 12 + 4 + 16 + 8 + 16 * 40
     assert ctypes.sizeof(tmc.CStatus) == 516
+    assert ctypes.sizeof(tmc.CAdamTensor) == 7 * 8 + 4 * 4  # seven pointers, rows, cols, decay, first block
 
 
 def test_version_and_defaults():

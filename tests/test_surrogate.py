@@ -176,6 +176,50 @@ def test_step_size_from_device_memory_and_fused_averaging_give_the_same_bits():
     assert torch.allclose(sums[0], dz.double().sum(0).float(), rtol=1e-4, atol=1e-3)
 
 
+def test_many_tensor_adam_equals_one_call_per_tensor():
+    """One launch over a table of parameter tensors (ragged sizes, some without bf16 copies or
+    averages) gives the same bits as one adam call per tensor."""
+    import ctypes
+
+    from tissuemc_b200 import surrogate as S
+
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    shapes = [(130, 257), (1, 513), (64, 64), (3, 1)]
+    sets = []
+    for _ in range(2):
+        torch.cuda.manual_seed(0)
+        sets.append([dict(w=torch.randn(r, c, device="cuda", generator=gen.manual_seed(7 + k)),
+                          g=torch.randn(r, c, device="cuda", generator=gen.manual_seed(70 + k)),
+                          m=torch.zeros(r, c, device="cuda"), v=torch.full((r, c), 0.5, device="cuda"),
+                          avg=torch.ones(r, c, device="cuda") if k % 2 == 0 else None,
+                          wb=torch.empty(r, c, dtype=torch.bfloat16, device="cuda") if k != 1 else None,
+                          wt=torch.empty(c, r, dtype=torch.bfloat16, device="cuda") if k != 1 else None)
+                     for k, (r, c) in enumerate(shapes)])
+    lr_dev = torch.tensor([2e-3], device="cuda")
+    for k, ((r, c), t) in enumerate(zip(shapes, sets[0], strict=True)):
+        S._call("tmc_b200_nn_adam", S._p(t["w"]), S._p(t["g"]), S._p(t["m"]), S._p(t["v"]), r, c, ctypes.c_float(0.0),
+                S._p(lr_dev), ctypes.c_float(0.9), ctypes.c_float(0.999), ctypes.c_float(1e-8),
+                ctypes.c_float(1e-4 * k), S._p(t["wb"]), S._p(t["wt"]), S._p(t["avg"]), ctypes.c_float(0.99), s)
+    rows = [tmc.CAdamTensor(t["w"].data_ptr(), t["g"].data_ptr(), t["m"].data_ptr(), t["v"].data_ptr(),
+                            0 if t["wb"] is None else t["wb"].data_ptr(), 0 if t["wt"] is None else t["wt"].data_ptr(),
+                            0 if t["avg"] is None else t["avg"].data_ptr(), r, c, 1e-4 * k, 0)
+            for k, ((r, c), t) in enumerate(zip(shapes, sets[1], strict=True))]
+    arr = (tmc.CAdamTensor * len(rows))(*rows)
+    blocks = tmc.lib().tmc_b200_nn_adam_plan(arr, len(rows))
+    assert blocks == sum((r * c + 255) // 256 for r, c in shapes)
+    assert [x.first_block for x in arr] == [0, 131, 134, 150]
+    dev = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8).cuda()
+    S._call("tmc_b200_nn_adam_multi", S._p(dev), len(rows), blocks, ctypes.c_float(0.0), S._p(lr_dev),
+            ctypes.c_float(0.9), ctypes.c_float(0.999), ctypes.c_float(1e-8), ctypes.c_float(0.99), s)
+    torch.cuda.synchronize()
+    for a, b in zip(sets[0], sets[1], strict=True):
+        for key in ("w", "m", "v", "avg", "wb", "wt"):
+            if a[key] is not None:
+                assert torch.equal(a[key], b[key]), key
+    assert tmc.lib().tmc_b200_nn_adam_plan(arr, 0) == -1
+
+
 def test_graph_captured_training_equals_host_launched_training():
     """Training with the optimiser step captured once as a CUDA graph and replayed gives the same
     weights and Adam moments, bit for bit, as launching every kernel from the host (the reported loss

@@ -117,6 +117,15 @@ class CSweepConfig(ctypes.Structure):
     ]
 
 
+class CAdamTensor(ctypes.Structure):
+    """tmc_adam_tensor: one parameter tensor of a many-tensor Adam step (device pointers)."""
+
+    _fields_ = [("w", ctypes.c_void_p), ("g", ctypes.c_void_p), ("m", ctypes.c_void_p), ("v", ctypes.c_void_p),
+                ("wb", ctypes.c_void_p), ("wt", ctypes.c_void_p), ("avg", ctypes.c_void_p),
+                ("rows", ctypes.c_int32), ("cols", ctypes.c_int32), ("weight_decay", ctypes.c_float),
+                ("first_block", ctypes.c_int32)]
+
+
 class CSweepOptions(ctypes.Structure):
     _fields_ = [("dz", ctypes.c_double), ("dr", ctypes.c_double)] + [
         (k, ctypes.c_int32) for k in ("nz", "nr", "na", "batches", "fast_math", "profiles", "device",
@@ -179,6 +188,9 @@ PROTOTYPES = {
                          [ctypes.c_float, ctypes.c_void_p] + [ctypes.c_float] * 4 + [ctypes.c_void_p] * 3 +
                          [ctypes.c_float, ctypes.c_void_p, _P(CStatus)]),
     "tmc_b200_nn_status": (ctypes.c_int, [ctypes.c_int32]),
+    "tmc_b200_nn_adam_plan": (ctypes.c_int32, [_P(CAdamTensor), ctypes.c_int32]),
+    "tmc_b200_nn_adam_multi": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
+                                              ctypes.c_void_p] + [ctypes.c_float] * 4 + [ctypes.c_void_p, _P(CStatus)]),
     "tmc_b200_nn_ema": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
                                        ctypes.c_void_p, _P(CStatus)]),
     "tmc_b200_nn_to_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,

@@ -226,16 +226,14 @@ __device__ __forceinline__ float polyak(float avg, float w, float beta) {
     return __fmaf_rn(beta, avg, __fmul_rn(__fsub_rn(1.0f, beta), w));
 }
 
-// Adam on float32 master weights (rows x cols, row-major), writing the bf16 copy and its transpose.
-// The step size is lr_dev[0] when lr_dev is given (so that a captured graph reads the current
-// step's value), else lr_t; with avg given, the averaged weights are updated from the new ones.
-__global__ void adam_kernel(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
-                            float *__restrict__ v, int rows, int cols, float lr_t, const float *__restrict__ lr_dev,
-                            float b1, float b2, float eps, float weight_decay, __nv_bfloat16 *wb,
-                            __nv_bfloat16 *wt, float *__restrict__ avg, float avg_beta) {
-    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= static_cast<size_t>(rows) * cols) return;
-    const float lr = lr_dev ? __ldg(lr_dev) : lr_t;
+// One Adam step of element i of a rows x cols float32 parameter (row-major): the moments, the
+// weight, its Polyak average (if avg), its bf16 copy (if wb) and transpose (if wt). Shared by the
+// one-tensor and the many-tensor kernels, so both give the same bits.
+__device__ __forceinline__ void adam_element(size_t i, float *__restrict__ w, const float *__restrict__ g,
+                                             float *__restrict__ m, float *__restrict__ v, int rows, int cols,
+                                             float lr, float b1, float b2, float eps, float weight_decay,
+                                             __nv_bfloat16 *wb, __nv_bfloat16 *wt, float *__restrict__ avg,
+                                             float avg_beta) {
     const float gi = g[i] + weight_decay * w[i];
     const float mi = b1 * m[i] + (1.0f - b1) * gi;
     const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
@@ -250,6 +248,39 @@ __global__ void adam_kernel(float *__restrict__ w, const float *__restrict__ g, 
         const int r = static_cast<int>(i / cols), c = static_cast<int>(i % cols);
         wt[static_cast<size_t>(c) * rows + r] = b;
     }
+}
+
+// Adam on float32 master weights (rows x cols, row-major), writing the bf16 copy and its transpose.
+// The step size is lr_dev[0] when lr_dev is given (so that a captured graph reads the current
+// step's value), else lr_t; with avg given, the averaged weights are updated from the new ones.
+__global__ void adam_kernel(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
+                            float *__restrict__ v, int rows, int cols, float lr_t, const float *__restrict__ lr_dev,
+                            float b1, float b2, float eps, float weight_decay, __nv_bfloat16 *wb,
+                            __nv_bfloat16 *wt, float *__restrict__ avg, float avg_beta) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= static_cast<size_t>(rows) * cols) return;
+    const float lr = lr_dev ? __ldg(lr_dev) : lr_t;
+    adam_element(i, w, g, m, v, rows, cols, lr, b1, b2, eps, weight_decay, wb, wt, avg, avg_beta);
+}
+
+constexpr int kAdamThreads = 256;
+
+// The same step for every tensor of a table (one launch for all of a network's parameters): block b
+// belongs to the tensor whose first_block range holds it.
+__global__ void adam_multi_kernel(const tmc_adam_tensor *__restrict__ tab, int count, float lr_t,
+                                  const float *__restrict__ lr_dev, float b1, float b2, float eps, float avg_beta) {
+    __shared__ tmc_adam_tensor T;
+    if (threadIdx.x == 0) {
+        int t = 0;
+        while (t + 1 < count && static_cast<int>(blockIdx.x) >= tab[t + 1].first_block) ++t;
+        T = tab[t];
+    }
+    __syncthreads();
+    const size_t i = static_cast<size_t>(static_cast<int>(blockIdx.x) - T.first_block) * kAdamThreads + threadIdx.x;
+    if (i >= static_cast<size_t>(T.rows) * T.cols) return;
+    const float lr = lr_dev ? __ldg(lr_dev) : lr_t;
+    adam_element(i, T.w, T.g, T.m, T.v, T.rows, T.cols, lr, b1, b2, eps, T.weight_decay,
+                 reinterpret_cast<__nv_bfloat16 *>(T.wb), reinterpret_cast<__nv_bfloat16 *>(T.wt), T.avg, avg_beta);
 }
 
 // D = sum over the splits of a split-K product's partials (fixed order: deterministic)
@@ -578,6 +609,30 @@ int tmc_b200_nn_adam(float *w, const float *g, float *m, float *v, int32_t rows,
     adam_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         w, g, m, v, rows, cols, lr_t, lr_dev, b1, b2, eps, weight_decay, reinterpret_cast<__nv_bfloat16 *>(wb),
         reinterpret_cast<__nv_bfloat16 *>(wt), avg, avg_beta);
+    return launched(st);
+}
+
+int32_t tmc_b200_nn_adam_plan(tmc_adam_tensor *tab, int32_t count) {
+    if (!tab || count < 1) return -1;
+    int64_t blocks = 0;
+    for (int t = 0; t < count; ++t) {
+        if (tab[t].rows < 1 || tab[t].cols < 1) return -1;
+        tab[t].first_block = static_cast<int32_t>(blocks);
+        blocks += (static_cast<int64_t>(tab[t].rows) * tab[t].cols + kAdamThreads - 1) / kAdamThreads;
+        if (blocks > 0x7FFFFFFF) return -1;
+    }
+    return static_cast<int32_t>(blocks);
+}
+
+int tmc_b200_nn_adam_multi(const tmc_adam_tensor *tab, int32_t count, int32_t blocks, float lr_t, const float *lr_dev,
+                           float b1, float b2, float eps, float avg_beta, void *stream, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (!tab || count < 1 || blocks < 1) {
+        put(st, TMC_BAD_ARGUMENT, "NULL table, no tensors or no blocks (plan the table first)");
+        return TMC_BAD_ARGUMENT;
+    }
+    adam_multi_kernel<<<static_cast<unsigned>(blocks), kAdamThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+        tab, count, lr_t, lr_dev, b1, b2, eps, avg_beta);
     return launched(st);
 }
 

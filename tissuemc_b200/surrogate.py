@@ -208,19 +208,39 @@ class Member:
 
     def adam(self, stream: int, lr_t: float = 0.0, lr_dev=None, b1=0.9, b2=0.999, eps=1e-8, wd=0.0, avg=None,
              ema: float = 0.0):
-        """One Adam step of every parameter. The bias-corrected step size is lr_t, or the float32
-        in device memory at lr_dev (a captured graph reads each step's value there). With avg =
-        (weights, biases) float32 copies, the Polyak average avg = ema avg + (1 - ema) w follows the
-        step in the same kernel."""
-        s = ctypes.c_void_p(stream)
+        """One Adam step of every parameter, in one launch over the member's parameter table. The
+        bias-corrected step size is lr_t, or the float32 in device memory at lr_dev (a captured
+        graph reads each step's value there). With avg = (weights, biases) float32 copies, the
+        Polyak average avg = ema avg + (1 - ema) w follows the step in the same kernel. Weight
+        decay applies to the weights, not the biases."""
+        tab, count, blocks = self._adam_table(wd, avg)
+        _call("tmc_b200_nn_adam_multi", _p(tab), count, blocks, ctypes.c_float(lr_t), _p(lr_dev), ctypes.c_float(b1),
+              ctypes.c_float(b2), ctypes.c_float(eps), ctypes.c_float(ema), ctypes.c_void_p(stream))
+
+    def _adam_table(self, wd: float, avg):
+        """The parameter table in device memory for these options (built once, then reused: a
+        captured graph keeps reading the same table)."""
         aw, ab = avg if avg is not None else ([None] * self.L, [None] * self.L)
-        for li, (k, n) in enumerate(LAYER_DIMS):
-            _call("tmc_b200_nn_adam", _p(self.W[li]), _p(self.gW[li]), _p(self.mW[li]), _p(self.vW[li]), n, k,
-                  ctypes.c_float(lr_t), _p(lr_dev), ctypes.c_float(b1), ctypes.c_float(b2), ctypes.c_float(eps),
-                  ctypes.c_float(wd), _p(self.Wb[li]), _p(self.WT[li]), _p(aw[li]), ctypes.c_float(ema), s)
-            _call("tmc_b200_nn_adam", _p(self.b[li]), _p(self.gb[li]), _p(self.mb[li]), _p(self.vb[li]), 1, n,
-                  ctypes.c_float(lr_t), _p(lr_dev), ctypes.c_float(b1), ctypes.c_float(b2), ctypes.c_float(eps),
-                  ctypes.c_float(0.0), _p(None), _p(None), _p(ab[li]), ctypes.c_float(ema), s)
+        key = (wd, tuple(0 if t is None else t.data_ptr() for t in list(aw) + list(ab)))
+        if getattr(self, "_adam_key", None) != key:
+            from . import CAdamTensor
+
+            rows = []
+            for li, (k, n) in enumerate(LAYER_DIMS):
+                rows.append(CAdamTensor(self.W[li].data_ptr(), self.gW[li].data_ptr(), self.mW[li].data_ptr(),
+                                        self.vW[li].data_ptr(), self.Wb[li].data_ptr(), self.WT[li].data_ptr(),
+                                        0 if aw[li] is None else aw[li].data_ptr(), n, k, wd, 0))
+                rows.append(CAdamTensor(self.b[li].data_ptr(), self.gb[li].data_ptr(), self.mb[li].data_ptr(),
+                                        self.vb[li].data_ptr(), 0, 0, 0 if ab[li] is None else ab[li].data_ptr(),
+                                        1, n, 0.0, 0))
+            arr = (CAdamTensor * len(rows))(*rows)
+            blocks = lib().tmc_b200_nn_adam_plan(arr, len(rows))
+            if blocks < 1:
+                raise RuntimeError("invalid Adam parameter table")
+            t = self.torch
+            dev = t.frombuffer(bytearray(bytes(arr)), dtype=t.uint8).to(self.dev)
+            self._adam_tab, self._adam_key = (dev, len(rows), blocks), key
+        return self._adam_tab
 
 
 @dataclass
@@ -261,7 +281,7 @@ class Ensemble:
         the weights at the end.
 
         One optimiser step of the whole ensemble (batch gathers, forward, backward, Adam and
-        averaging: 46 launches per member) runs once from the host and is then captured as a
+        averaging: 37 launches per member) runs once from the host and is then captured as a
         CUDA graph, one independent branch per member, that every later step replays; each step's
         batch indices and step size reach the graph through device buffers written before the
         replay. graph=False launches every kernel from the host, one member after the other. Both
