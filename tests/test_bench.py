@@ -1,5 +1,6 @@
-"""bench.py on the CPU: the reference arm's JSON line (it times the reference's own CPU engine)
-and the clock-sample parser that flags throttled runs."""
+"""bench.py on the CPU: the reference arm's JSON line (it times the reference's own CPU engine),
+the clock-sample parser that flags throttled runs, and the roofline peaks (measured or
+fallback)."""
 
 from __future__ import annotations
 
@@ -44,3 +45,17 @@ def test_clock_summary_reads_throttle_reasons():
     assert s["reasons"] == ["sw_power_cap"]
     c.lines = ["0, 900, 1965, 400.0, 0x8, Active, Not Active, Active, Not Active"]
     assert c.summary()["reasons"] == ["hw_slowdown", "sw_thermal_slowdown"]
+
+
+def test_roofline_peaks_say_whether_they_were_measured(tmp_path, monkeypatch):
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    monkeypatch.setattr(bench, "ROOT", tmp_path)
+    value, note = bench._peak("bf16_tflops", 1590.0)
+    assert value == 1590.0 and "fallback" in note
+    (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"gemm": {"bf16_tflops": 1651.9}, "hbm_gbs": 6650}))
+    value, note = bench._peak("bf16_tflops", 1590.0)
+    assert value == 1651.9 and "measured" in note
+    assert bench._peak("hbm_gbs", 1.0) == (6650.0, "hbm_gbs of MEASURED_PEAKS.json (measured)")
+    assert bench._peak("sm_max_mhz", 1965.0)[1].startswith("fallback")
