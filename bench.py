@@ -82,6 +82,8 @@ def _args():
     ap.add_argument("--photon-scale", type=float, default=1.0, help="sweep: scale every configuration's photons "
                     "(diagnostic)")
     ap.add_argument("--no-loop", action="store_true", help="sweep: skip the single-run loop baseline (diagnostic)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default line only: skip the sweep, serve and reference-GPU sub-measurements")
     ap.add_argument("--no-profiles", action="store_true",
                     help="diagnostic: skip the profile tallies (rung 6 without profiles); not a result")
     return ap.parse_args()
@@ -209,6 +211,39 @@ def reference_cpu_sample(workload: str, target_s: float = 12.0) -> dict:
                       f"oracle/_ref/tissuemc, {r['threads']} threads on {model})"}
 
 
+REF_GPU_BIN = ROOT / "baseline" / "_ref" / "tissuemc_cuda"
+
+
+def reference_gpu_run(workload: str, photons: int, batches: int, rung: int = 7, repeats: int = 2) -> dict:
+    """The reference's own CUDA engine (TissueMC's src/cuda/engine.cu at rung `rung`, compiled
+    unchanged for sm_100a into baseline/_ref/tissuemc_cuda by baseline/Makefile) on the same
+    workload, photons, batches and seed on this GPU, timed by its own kernel_seconds (CUDA events
+    around its kernels, src/cuda/engine.cu:209-275); the mean of `repeats` runs after one warm-up."""
+    import tempfile
+
+    if not REF_GPU_BIN.exists():
+        return {"unavailable": "baseline/_ref/tissuemc_cuda is not built (make -C baseline needs the TissueMC sources)"}
+    mci = ROOT / "tissuemc_b200" / "configs" / f"{workload}.mci"
+    ks, ws = [], []
+    with tempfile.TemporaryDirectory() as tmp:
+        out = Path(tmp) / "ref.json"
+        for i in range(repeats + 1):
+            p = subprocess.run([str(REF_GPU_BIN), "run", str(mci), "--engine", "cuda", "--rung", str(rung),
+                                "--photons", str(photons), "--batches", str(batches), "--seed", "1",
+                                "--output", str(out)], capture_output=True, text=True, timeout=900)
+            if p.returncode != 0:
+                return {"unavailable": f"the reference's CUDA engine exited {p.returncode}: {p.stderr.strip()[:200]}"}
+            r = json.loads(out.read_text())["runs"][0]
+            if i:
+                ks.append(float(r["kernel_seconds"]))
+                ws.append(float(r["wall_seconds"]))
+    k = sum(ks) / len(ks)
+    return {"value": photons / k, "unit": "photons/s", "rung": rung, "kernel_seconds": k,
+            "wall_seconds": sum(ws) / len(ws), "photons": photons, "batches": batches, "repeats": repeats,
+            "what": f"TissueMC's own CUDA engine, rung {rung}, compiled unchanged for sm_100a "
+                    "(baseline/_ref/tissuemc_cuda), its kernel_seconds on this GPU"}
+
+
 def run_reference_arm(a) -> None:
     rank, world, _ = _dist()
     if rank != 0:
@@ -232,52 +267,87 @@ def run_reference_arm(a) -> None:
     print(json.dumps(line), flush=True)
 
 
-def run_sweep(a) -> None:
-    """Batched sweep: solves/s of the graph-captured persistent launch, beside the loop of
-    single-run launches over the same configurations (equal total photons)."""
-    import time
+# Interaction and boundary steps per photon of the 4096-configuration sweep workload, weighted by
+# the configurations' photon counts (float64 oracle, 128 photons of each configuration).
+SWEEP_STEPS_PER_PHOTON = (141.1, 3.8)
 
+
+def issue_roofline(steps: tuple[float, float], n_sm: int, f_mhz: float) -> tuple[float, str, float, float]:
+    """Photons/s of the FP32/SFU issue roofline for a photon of `steps` (interaction, boundary)
+    steps: N_SM x f / max(F / 128, S / 16) with the frozen per-step counts F_*, S_*; returns the
+    bound, which term binds, and F, S per photon."""
+    f_tot = steps[0] * F_INT + steps[1] * F_BND
+    s_tot = steps[0] * S_INT + steps[1] * S_BND
+    clocks_per_photon = max(f_tot / 128.0, s_tot / 16.0) / n_sm
+    return f_mhz * 1e6 / clocks_per_photon, ("sfu" if s_tot / 16.0 >= f_tot / 128.0 else "fp32"), f_tot, s_tot
+
+
+def measure_sweep(configs: int, steps: int, warmup: int, device: int, seed: int = 1, autotune: bool = False,
+                  photon_scale: float = 1.0, loop: bool = True) -> dict:
+    """Batched sweep: solves/s of the graph-captured persistent launch (CUDA events around the sweep
+    kernel, tmc_b200_sweep_run's kernel_seconds) and end to end (host clock around the call: table
+    upload, the launch, the summary download), beside a loop of single-run launches over the same
+    configurations (equal total photons)."""
     import tissuemc_b200 as tmc
 
-    rank, world, local = _dist()
-    cfgs = tmc.sweep_sample(1 + rank, a.configs)
-    if a.photon_scale != 1.0:  # diagnostic: a shorter sweep over the same configurations
+    cfgs = tmc.sweep_sample(seed, configs)
+    if photon_scale != 1.0:  # diagnostic: a shorter sweep over the same configurations
         for c in cfgs:
-            c.photons = max(1, int(c.photons * a.photon_scale))
-    opt = tmc.sweep_options(device=local)
-    if a.autotune:
+            c.photons = max(1, int(c.photons * photon_scale))
+    opt = tmc.sweep_options(device=device)
+    if autotune:
         opt, _ = tmc.sweep_autotune(cfgs, opt)
-    for _ in range(a.warmup):
+    for _ in range(warmup):
         tmc.sweep_run(cfgs, opt)
-    with Clocks(local) as clk:
+    with Clocks(device) as clk:
         kern, wall = [], []
-        for _ in range(a.steps):
+        for _ in range(steps):
             t0 = time.perf_counter()
             r = tmc.sweep_run(cfgs, opt)
             wall.append(time.perf_counter() - t0)
             kern.append(r.seconds)
-    loop = None if a.no_loop else tmc.sweep_run_loop(cfgs, opt).seconds
+    loop_s = tmc.sweep_run_loop(cfgs, opt).seconds if loop else None
     n = len(cfgs)
     ks, ws = sum(kern) / len(kern), sum(wall) / len(wall)
+    photons = sum(int(c.photons) for c in cfgs)
+    import torch
+
+    n_sm = torch.cuda.get_device_properties(device).multi_processor_count
+    f_mhz, f_note = _peak("sm_max_mhz", 1965.0)
+    peak, bound, f_tot, s_tot = issue_roofline(SWEEP_STEPS_PER_PHOTON, n_sm, f_mhz)
+    return {
+        "metric": "solves/s on 1 B200 (batched sweep)", "value": n / ks, "unit": "solves/s",
+        "ms_per_step": 1e3 * ks, "steps": steps, "warmup": warmup,
+        "config": {"workload": f"sweep: {SWEEP_DESC}", "configs": n, "photon_scale": photon_scale,
+                   "threads_per_block": opt.threads_per_block, "item_photons": opt.item_photons,
+                   "autotuned": bool(autotune)},
+        "e2e": {"value": n / ws, "unit": "solves/s",
+                "h2d_bytes_per_step": n * 48 + n * 4 + sum(c.num_layers for c in cfgs) * 96,
+                "d2h_bytes_per_step": n * (opt.nr + 3) * 8},
+        "loop_baseline": None if loop_s is None else {
+            "value": n / loop_s, "unit": "solves/s", "seconds": loop_s,
+            "what": "one single-run walk launch per configuration, back to back on one stream"},
+        "speedup_vs_loop": None if loop_s is None else loop_s / ks,
+        "photons_per_s": photons / ks,
+        "roofline": {"bound": bound, "achieved": photons / ks / 1e9, "peak": peak / 1e9, "unit": "Gphotons/s",
+                     "frac": photons / ks / peak,
+                     "peak_source": f"issue roofline: {n_sm} SMs x {f_mhz:.0f} MHz ({f_note}) / max(F/128, S/16), "
+                                    f"F={f_tot:.0f} FP32 and S={s_tot:.0f} SFU ops per photon"},
+        "gpu_launches": steps * 2, "clocks": clk.summary(),
+    }
+
+
+def run_sweep(a) -> None:
+    rank, world, local = _dist()
+    m = measure_sweep(a.configs, a.steps, a.warmup, local, seed=1 + rank, autotune=a.autotune,
+                      photon_scale=a.photon_scale, loop=not a.no_loop)
     if rank == 0:
-        print(json.dumps({
-            "metric": "solves/s on 1 B200 (batched sweep)", "value": world * n / ks, "unit": "solves/s",
-            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * ks,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 transport, u64 fixed-point tallies", "data": "synthetic (seeded configurations)",
-            "config": {"workload": f"sweep: {SWEEP_DESC}", "configs": n, "photon_scale": a.photon_scale,
-                       "threads_per_block": opt.threads_per_block,
-                       "item_photons": opt.item_photons, "autotuned": bool(a.autotune)},
-            "e2e": {"value": world * n / ws, "unit": "solves/s",
-                    "h2d_bytes_per_step": n * 48 + n * 4 + sum(c.num_layers for c in cfgs) * 96,
-                    "d2h_bytes_per_step": n * (opt.nr + 3) * 8},
-            "loop_baseline": None if loop is None else {
-                "value": n / loop, "unit": "solves/s", "seconds": loop,
-                "what": "one single-run walk launch per configuration, back to back on one stream"},
-            "speedup_vs_loop": None if loop is None else loop / ks,
-            "photons_per_s": sum(int(c.photons) for c in cfgs) / ks,
-            "gpu_launches": a.steps * 2, "clocks": clk.summary(),
-        }), flush=True)
+        line = {"metric": m["metric"], "value": world * m["value"], "unit": "solves/s", "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32 transport, u64 fixed-point tallies",
+                "data": "synthetic (seeded configurations)"}
+        line.update({k: v for k, v in m.items() if k not in line})
+        print(json.dumps(line), flush=True)
 
 
 def run_surrogate(a) -> None:
@@ -297,29 +367,28 @@ def run_surrogate(a) -> None:
             "speedup_vs_plain_mc": s["speedup_vs_plain_mc"], "details": res}), flush=True)
 
 
-def run_serve(a) -> None:
-    """Surrogate serving throughput: one fused tcgen05 launch (tmc_b200_nn_ensemble_infer) per
-    step over --queries feature vectors drawn from the sweep distribution. The weights are random
-    (the kernel's work does not depend on their values). value = queries / CUDA-event time of the
-    launch, L2 flushed between steps; e2e = queries / host time of FusedServer (pinned host
-    features in, host outputs, mean R_d and route flags out)."""
+def measure_serve(queries: int, steps: int, warmup: int, device: int, seed: int = 3000) -> dict:
+    """Surrogate serving throughput: one fused tcgen05 launch (tmc_b200_nn_ensemble_infer) per step
+    over `queries` feature vectors drawn from the sweep distribution. The weights are random (the
+    kernel's work does not depend on their values). value = queries / CUDA-event time of the launch,
+    L2 flushed between steps; e2e = queries / host time of FusedServer (pinned host features in,
+    host outputs, mean R_d and route flags out)."""
     import numpy as np
     import torch
 
     import tissuemc_b200 as tmc
     from tissuemc_b200 import surrogate as S
 
-    rank, world, local = _dist()
-    torch.cuda.set_device(local)
-    n = a.queries
-    ens = S.Ensemble(members=4, batch=4096, seed=0, device=f"cuda:{local}")
+    torch.cuda.set_device(device)
+    n = queries
+    ens = S.Ensemble(members=4, batch=4096, seed=0, device=f"cuda:{device}")
     ens.norm = S.Norm(np.zeros(S.N_FEAT), np.ones(S.N_FEAT), np.full(S.N_OUT, -2.0), np.full(S.N_OUT, 0.3))
-    q = S.features(tmc.sweep_sample(3000 + rank, n))
+    q = S.features(tmc.sweep_sample(seed, n))
     q = (q - q.mean(0)) / np.maximum(q.std(0), 1e-6)
     fs = S.FusedServer(ens)
     fs._reserve(n)
     fs.d_feats[:n].copy_(torch.from_numpy(q.astype(np.float32)))
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
     stream = torch.cuda.current_stream()
 
     def step() -> float:
@@ -331,41 +400,51 @@ def run_serve(a) -> None:
         e1.synchronize()
         return e0.elapsed_time(e1)
 
-    for _ in range(a.warmup):
+    for _ in range(warmup):
         step()
-    with Clocks(local) as clk:
-        times = [step() for _ in range(a.steps)]
+    with Clocks(device) as clk:
+        times = [step() for _ in range(steps)]
     if tmc.lib().tmc_b200_nn_status(1):
         raise RuntimeError("a tensor-core wait gave up in the fused ensemble kernel")
     ms = sum(times) / len(times)
     # end to end: features already in pinned host memory, results back in pinned host memory
     h_q = torch.from_numpy(q.astype(np.float32)).pin_memory()
     e2e_t = []
-    for i in range(a.steps + 1):
+    for i in range(steps + 1):
         t0 = time.perf_counter()
         fs(h_q, copy=False)
         if i:
             e2e_t.append(time.perf_counter() - t0)
     e2e_s = sum(e2e_t) / len(e2e_t)
+    peak, peak_note = _peak("bf16_tflops", 1590.0)
+    achieved = n * SERVE_FLOP_PER_QUERY / (ms * 1e-3) / 1e12
+    del flush
+    return {
+        "metric": "surrogate queries/s on 1 B200 (fused ensemble kernel)", "value": n / (ms * 1e-3),
+        "unit": "queries/s", "ms_per_step": ms, "steps": steps, "warmup": warmup,
+        "dtype": "bf16 operands, fp32 accumulation",
+        "config": {"workload": f"serve: {WORKLOADS['serve']}", "queries_per_step": n,
+                   "l2": "flushed between steps (256 MB write)"},
+        "e2e": {"value": n / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": n * S.N_FEAT * 4,
+                "d2h_bytes_per_step": n * (S.N_OUT * 4 + 4 + 1)},
+        "gpu_launches": steps,
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": f"bf16 burst peak: {peak_note}; algorithmic FLOPs of the "
+                                    "padded layers, 7.08 MFLOP per query"},
+        "clocks": clk.summary(),
+    }
+
+
+def run_serve(a) -> None:
+    rank, world, local = _dist()
+    m = measure_serve(a.queries, a.steps, a.warmup, local, seed=3000 + rank)
     if rank == 0:
-        peak, peak_note = _peak("bf16_tflops", 1590.0)
-        achieved = n * SERVE_FLOP_PER_QUERY / (ms * 1e-3) / 1e12
-        print(json.dumps({
-            "metric": "surrogate queries/s on 1 B200 (fused ensemble kernel)", "value": n / (ms * 1e-3),
-            "unit": "queries/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "bf16 operands, fp32 accumulation", "data": "synthetic (sweep-distribution queries, random weights)",
-            "config": {"workload": f"serve: {WORKLOADS['serve']}", "queries_per_step": n,
-                       "l2": "flushed between steps (256 MB write)"},
-            "e2e": {"value": n / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": n * S.N_FEAT * 4,
-                    "d2h_bytes_per_step": n * (S.N_OUT * 4 + 4 + 1)},
-            "gpu_launches": a.steps,
-            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "peak_source": f"bf16 burst peak: {peak_note}; algorithmic FLOPs of the "
-                                        "padded layers, 7.08 MFLOP per query"},
-            "clocks": clk.summary(),
-        }), flush=True)
+        line = {"metric": m["metric"], "value": m["value"], "unit": "queries/s", "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "data": "synthetic (sweep-distribution queries, random weights)"}
+        line.update({k: v for k, v in m.items() if k not in line})
+        print(json.dumps(line), flush=True)
 
 
 def run_train(a) -> None:
@@ -452,8 +531,10 @@ def main() -> None:
     first, count = tmc.shard_range(spec.photons, rank, world)
     opt = tmc.options(batches=a.batches, seed=1, device=local, rung=6 if a.no_profiles else 0,
                       profiles=not a.no_profiles)
-    words = int(tmc.query_sizes(spec, opt).tally_words)
-    d_tally = torch.empty(words, dtype=torch.int64, device=f"cuda:{local}")
+    sizes = tmc.query_sizes(spec, opt)
+    words = int(sizes.tally_words)
+    # the tallies, then the launch's photon-claim counter (device_words = tally_words + 1)
+    d_tally = torch.empty(int(sizes.device_words), dtype=torch.int64, device=f"cuda:{local}")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     stream = torch.cuda.Stream(device=local)
 
@@ -513,7 +594,7 @@ def main() -> None:
             with torch.cuda.stream(stream):
                 walk()
             stream.synchronize()  # the walk and the all-reduce ran on `stream`, not the current one
-            host = d_tally.cpu()
+            host = d_tally[:words].cpu()
             res = tmc.decode(spec, opt, host.numpy().view(np.uint64))
             res.device = torch.cuda.get_device_name(local)
         if i:  # the first call is a warm-up
@@ -532,11 +613,7 @@ def main() -> None:
     if rank == 0:
         f_mhz, f_note = _peak("sm_max_mhz", 1965.0)
         n_sm = torch.cuda.get_device_properties(local).multi_processor_count
-        e_int, e_bnd = STEPS_PER_PHOTON[a.workload]
-        f_tot = e_int * F_INT + e_bnd * F_BND
-        s_tot = e_int * S_INT + e_bnd * S_BND
-        clocks_per_photon = max(f_tot / 128.0, s_tot / 16.0) / n_sm  # SM-clocks per photon, whole GPU
-        peak = f_mhz * 1e6 / clocks_per_photon
+        peak, bound, f_tot, s_tot = issue_roofline(STEPS_PER_PHOTON[a.workload], n_sm, f_mhz)
         achieved = photons / (ms / 1e3)
         line = {
             "metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": world, "steps": a.steps,
@@ -551,7 +628,7 @@ def main() -> None:
             "e2e": e2e,
             "gpu_launches": a.steps,
             "roofline": {
-                "bound": "sfu" if s_tot / 16.0 >= f_tot / 128.0 else "fp32", "achieved": achieved / 1e9,
+                "bound": bound, "achieved": achieved / 1e9,
                 "peak": peak / 1e9, "unit": "Gphotons/s", "frac": achieved / peak,
                 "traffic": WALK_DRAM_BYTES.get(a.workload) if not a.photons else None,
                 "peak_source": f"issue roofline: {n_sm} SMs x {f_mhz:.0f} MHz ({f_note}) / "
@@ -567,6 +644,20 @@ def main() -> None:
                 line["cpu_baseline"].pop("seconds", None)
             except Exception as exc:  # report, never fake
                 line["cpu_baseline"] = {"unavailable": str(exc)}
+        if world == 1 and not a.no_extras and not a.photons:
+            # the other parts of the metric, measured in the same run on the same GPU: the batched
+            # sweep (solves/s vs the loop of plain launches), the gated surrogate's serving kernel,
+            # and the reference's own CUDA engine on this workload
+            ref_gpu = reference_gpu_run(a.workload, spec.photons, a.batches)
+            if "value" in ref_gpu:
+                ref_gpu["b200_kernel_speedup"] = value / ref_gpu["value"]
+            line["reference_gpu"] = ref_gpu
+            for key, fn in (("sweep", lambda: measure_sweep(4096, 2, 1, local)),
+                            ("serve", lambda: measure_serve(1 << 20, 5, 3, local))):
+                try:
+                    line[key] = fn()
+                except Exception as exc:  # report, never fake
+                    line[key] = {"unavailable": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

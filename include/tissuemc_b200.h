@@ -40,7 +40,7 @@ extern "C" {
 #endif
 
 #define TMC_B200_MAX_LAYERS 16
-#define TMC_B200_ABI_VERSION 1
+#define TMC_B200_ABI_VERSION 2
 
 typedef enum {
     TMC_OK = 0,
@@ -87,6 +87,9 @@ typedef struct {
     int32_t threads_per_block; /* 0 = chosen by the planner                                     */
     int32_t blocks_per_sm;     /* 0 = chosen by the planner                                     */
     int32_t smem_budget;       /* bytes of shared memory per block for tallies; 0 = planner     */
+    uint32_t step_cap;         /* a packet still alive after this many steps is ended and counted
+                                  as an anomaly (0 = 2,000,000,000); no reference counterpart: the
+                                  reference loops until the packet dies (physics.hpp:279-287) */
 } tmc_options;
 
 /* Element counts of every output buffer for a run (tmc_b200_query_sizes). */
@@ -96,6 +99,9 @@ typedef struct {
     uint64_t a_rz;     /* nr * nz  */
     uint64_t ra;       /* nr * na  (each of rd_ra and tt_ra) */
     uint64_t tally_words; /* 64-bit words of the raw fixed-point tally buffer */
+    uint64_t device_words; /* 64-bit words of the device buffer of tmc_b200_run_device and
+                              tmc_b200_run_device_range: the tally words, then one word that holds
+                              the call's photon-claim counter */
 } tmc_sizes;
 
 /* Caller-allocated host buffers for one run. Every pointer is required unless marked optional.
@@ -146,10 +152,12 @@ TMC_B200_API int tmc_b200_query_sizes(const tmc_run_spec *spec, const tmc_option
 TMC_B200_API int tmc_b200_run(const tmc_run_spec *spec, const tmc_options *opt, tmc_result *result,
                  tmc_status *status);
 
-/* Device-resident variant for callers that keep the tallies on the GPU: zeroes the fixed-point
- * tally buffer `d_tally` (device memory, tally_words 64-bit words), runs the walk on `stream`
- * (a cudaStream_t, NULL = the legacy default stream) and returns without synchronising.
- * `kernel_ms` (optional, host) receives nothing here; time with events on `stream`. */
+/* Device-resident variant for callers that keep the tallies on the GPU: zeroes the buffer
+ * `d_tally` (device memory, tmc_sizes.device_words 64-bit words: the tally_words fixed-point
+ * tallies, then the launch's photon-claim counter), runs the walk on `stream` (a cudaStream_t,
+ * NULL = the legacy default stream) and returns without synchronising; time it with events on
+ * `stream`. Everything the launch writes is in `d_tally`, so calls on different streams into
+ * different buffers may run at the same time on the GPU. */
 TMC_B200_API int tmc_b200_run_device(const tmc_run_spec *spec, const tmc_options *opt, uint64_t *d_tally,
                         void *stream, tmc_status *status);
 
@@ -187,9 +195,10 @@ TMC_B200_API int tmc_b200_plan(const tmc_run_spec *spec, const tmc_options *opt,
 #define TMC_B200_STATIC_SCRATCH_WORDS 65536u
 
 /* Run the walk without allocating anything. No counterpart in the reference: it exists for callers
- * that cannot call cudaMalloc, such as a host program that runs while a stream is being captured
- * into a CUDA graph (allocation is not permitted then) or a framework that owns all device memory
- * through its own pool. Results are as tmc_b200_run's, bit for bit.
+ * that cannot call cudaMalloc — a framework that owns every byte of device memory through its own
+ * pool and does not let libraries allocate behind its back, or a plugin host that hands its
+ * plugins a fixed memory budget and counts any cudaMalloc against them as a failure. Results are
+ * as tmc_b200_run's, bit for bit.
  *
  * The walk's scratch (its photon-claim counter and the fixed-point tally accumulators) lives in a
  * static device array of the library, TMC_B200_STATIC_SCRATCH_WORDS words plus a 256-byte head,
@@ -199,11 +208,14 @@ TMC_B200_API int tmc_b200_plan(const tmc_run_spec *spec, const tmc_options *opt,
  * and is then decoded into the other arrays. No cudaMalloc, cudaFree, stream or event creation,
  * and no host-side allocation on success.
  *
- * The first call on a device sets up that device (the array's device address, the kernels'
- * shared-memory limit); make it before any stream capture begins. Each call clears the parts of
- * the array it uses and runs on the legacy default stream, synchronously. Every call shares the
- * one array: calls serialise on the host, and calls that could overlap on the GPU (from other
- * code paths on other streams) would race. kernel_seconds is measured by the host clock here. */
+ * The first call on a device sets up that device (it looks up the array's device address and
+ * raises the kernels' shared-memory limit). Each call clears the parts of the array it uses,
+ * runs on the legacy default stream (which waits for, and is waited on by, the blocking streams
+ * of the device) and returns when the tallies are in result->raw. The calling thread's current
+ * device is the same on return as on entry. Every call shares the one array: calls serialise on
+ * the host, and calls that could overlap on the GPU (from other code paths on other streams)
+ * would race. kernel_seconds is host time from the launch to the end of the walk (a stream
+ * synchronisation), without the copy of the tallies. */
 TMC_B200_API int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_result *result,
                                      tmc_status *status);
 
@@ -286,6 +298,15 @@ TMC_B200_API int tmc_b200_sweep_autotune(const tmc_sweep_config *cfgs, int32_t n
  * bounded tensor-core wait gave up. */
 TMC_B200_API int tmc_b200_gemm_bf16(const uint16_t *A, const uint16_t *B, const float *bias, float *D, int32_t M,
                                     int32_t N, int32_t K, void *stream, tmc_status *status);
+
+/* Test of a bounded device wait that gives up (no counterpart in the reference). Runs the GEMM
+ * kernel above on one 128 x 128 x 64 product (a few KB of device memory, allocated and freed here)
+ * with its producer told to issue no loads, so that the MMA issuer's wait on a stage nobody fills
+ * runs out after wait_limit polls (1 .. the production limit) with no copy and no MMA outstanding.
+ * The kernel then skips its epilogue, frees its tensor memory and raises its status word. Returns
+ * TMC_DEVICE_TIMEOUT when the status word reported the give-up (the expected result), TMC_OK if it
+ * did not; the device stays usable either way. Synchronous. */
+TMC_B200_API int tmc_b200_probe_wait_timeout(int32_t device, uint32_t wait_limit, tmc_status *status);
 
 /* ------------------------------------------------------------------ surrogate network ops
  * The learned surrogate's building blocks (no counterpart in the reference). Device pointers of

@@ -28,7 +28,6 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liboracle.so"
 REF_BIN = HERE / "_ref" / "tissuemc"
-REF_CUDA_BIN = HERE / "_ref" / "tissuemc_cuda"
 
 MAX_LAYERS = 16
 

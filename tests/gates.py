@@ -7,8 +7,13 @@
   relative, events <= 1e-3 relative, no anomalies, profile totals <= 1e-4 relative, cumulative
   profile shape <= 1e-3 of the total), applied to a_z and rd_r as the reference applies them, and
   extended here to T_t(r) and to the flattened 2-D tallies A(r,z), R_d(r,a), T_t(r,a).
-* ``bin_z_scores`` — per-bin |z| between two runs for every bin above a count floor, with each
-  bin's standard error from the spread of its per-batch sums.
+* ``bin_z_scores`` — per-bin |z| between two runs of the same photons for every bin above a count
+  floor, with each bin's standard error from the spread of the reference run's per-batch sums.
+* ``per_photon_bins`` / ``bin_z_two_runs`` — per-bin |z| between two runs of any photon counts, each
+  side with its own standard error from its own per-batch sums (the reference's batch estimate,
+  src/io/json_out.cpp:37-64, applied to every bin); ``family_check`` judges the |z| of many
+  independent bins at once (a fixed |z| < 3 on every one of 10^4-10^5 independent bins fails by
+  chance alone: 0.3 % of them exceed 3 under the null).
 * ``conservation`` — validate.py:134-153: the residual of R_d + T_t + A + R_sp - 1 within 3 SE plus
   a floor (1e-6 for float32 transport).
 """
@@ -148,15 +153,82 @@ def identical_photon_gaps(a: Run, b: Run, profiles=("a_z", "rd_r", "tt_r", "a_rz
 
 def bin_z_scores(ours: np.ndarray, ref: np.ndarray, ref_batches: np.ndarray, counts: np.ndarray,
                  floor: int) -> tuple[np.ndarray, int]:
-    """|z| per bin with >= floor contributing scores. The standard error of a bin's total is the
-    standard error of its per-batch sums (ref_batches: (B, bins)) times B; ours is assumed to have
-    the same variance (same photons, same physics), so the gap's SE is sqrt(2) times that."""
+    """|z| per bin with >= floor contributing scores, for two runs of the SAME photons and batches.
+    The standard error of a bin's total is the standard error of the reference run's per-batch sums
+    (ref_batches: (B, bins)) times B; the other run has the same photons, hence the same variance,
+    so the gap's SE is taken as sqrt(2) times that. For runs of different photons use
+    bin_z_two_runs."""
     b = ref_batches.shape[0]
     se_total = ref_batches.std(axis=0, ddof=1) * math.sqrt(b)
     mask = counts >= floor
     se = np.sqrt(2.0) * se_total[mask]
     z = np.abs(ours[mask] - ref[mask]) / np.where(se > 0, se, np.inf)
     return z, int(mask.sum())
+
+
+def per_photon_bins(batches: np.ndarray, photons: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Per-photon mean of every bin and its standard error from per-batch sums: batches is (B, bins)
+    summed weight, photons (B,) photons per batch. The mean is the total over all photons; the SE is
+    the sample standard deviation of the per-batch per-photon values over sqrt(B), as the reference
+    estimates R_d, T_t and A (src/io/json_out.cpp:37-64)."""
+    batches = np.asarray(batches, dtype=np.float64)
+    n = np.asarray(photons, dtype=np.float64)
+    b = batches.shape[0]
+    mean = batches.sum(axis=0) / n.sum()
+    se = (batches / n[:, None]).std(axis=0, ddof=1) / math.sqrt(b)
+    return mean, se
+
+
+def bin_z_two_runs(a_batches: np.ndarray, a_photons: np.ndarray, b_batches: np.ndarray, b_photons: np.ndarray,
+                   counts: np.ndarray, floor: int) -> tuple[np.ndarray, int]:
+    """|z| per bin with >= floor contributing scores (counts: of either run) between two runs of any
+    photon counts: the difference of the per-photon means over the root sum of squares of the two
+    standard errors, each from its own run's per-batch sums."""
+    ma, sa = per_photon_bins(a_batches, a_photons)
+    mb, sb = per_photon_bins(b_batches, b_photons)
+    mask = np.asarray(counts).ravel() >= floor
+    se = np.hypot(sa, sb)[mask]
+    z = np.abs(ma - mb)[mask] / np.where(se > 0, se, np.inf)
+    return z, int(mask.sum())
+
+
+@dataclass(frozen=True)
+class Family:
+    """Verdict on the |z| of n independent bins: the count above 3 against its null expectation,
+    and the largest |z| against the bound that n independent Student-t draws stay under with
+    probability 1 - alpha (Bonferroni)."""
+
+    n: int
+    over3: int
+    over3_limit: float
+    zmax: float
+    zmax_limit: float
+
+    @property
+    def passed(self) -> bool:
+        return self.over3 <= self.over3_limit and self.zmax < self.zmax_limit
+
+    def __str__(self) -> str:
+        return (f"[{'PASS' if self.passed else 'FAIL'}] {self.n} bins: {self.over3} with |z| > 3 "
+                f"(limit {self.over3_limit:.0f}), max |z| {self.zmax:.2f} (limit {self.zmax_limit:.2f})")
+
+
+def family_check(z: np.ndarray, dof: int, alpha: float = 1e-3) -> Family:
+    """Judge |z| of independent bins whose standard errors come from `dof` + 1 batches. Under the
+    null, |z| follows Student's t with about `dof` degrees of freedom: P(|z| > 3) = p3; the count
+    above 3 may exceed n p3 by twice itself plus five binomial standard deviations (the SE estimates
+    of neighbouring bins are correlated through shared photons), and the maximum must stay below
+    the two-sided 1 - alpha / n quantile."""
+    from scipy import stats
+
+    z = np.asarray(z, dtype=np.float64)
+    n = int(z.size)
+    if n == 0:
+        return Family(0, 0, 0.0, 0.0, math.inf)
+    p3 = 2.0 * float(stats.t.sf(3.0, dof))
+    limit3 = 2.0 * n * p3 + 5.0 * math.sqrt(n * p3 * (1 - p3))
+    zlim = float(stats.t.isf(alpha / (2.0 * n), dof))
+    return Family(n, int((z > 3.0).sum()), limit3, float(z.max()), zlim)
 
 
 def conservation(run: Run, precision: str = "float32") -> tuple[float, float, bool]:

@@ -1,7 +1,7 @@
 """Regenerate the golden fixtures in tests/golden/ from the TissueMC reference (run in a container
 that has the reference sources; the GPU box never reads them).
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref PATH]   (default: a `reference` directory beside the repo)
 
 Writes:
   philox_kat.json     the Random123 known-answer vectors quoted in the reference's
@@ -72,7 +72,7 @@ def slim(run: dict) -> dict:
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", type=Path, default=Path("/root/reference"))
+    ap.add_argument("--ref", type=Path, default=ROOT.parent / "reference")
     args = ap.parse_args()
     ref = args.ref
     subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), f"REF={ref}"], check=True)

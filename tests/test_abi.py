@@ -50,7 +50,7 @@ def test_struct_sizes_match_the_header_layout():
 
 def test_version_and_defaults():
     lib = tmc.lib()
-    assert lib.tmc_b200_abi_version() == 1
+    assert lib.tmc_b200_abi_version() == 2
     assert b"sm_100a" in lib.tmc_b200_version()
     o = tmc.COptions()
     lib.tmc_b200_default_options(ctypes.byref(o))
@@ -96,6 +96,7 @@ def test_query_sizes():
     assert (sz.batches, sz.layers, sz.nz, sz.nr, sz.na) == (4, 2, 7, 5, 3)
     assert (sz.absorbed, sz.a_rz, sz.ra) == (8, 35, 15)
     assert sz.tally_words == 4 * (4 + 2) + 35 + 2 * 15
+    assert sz.device_words == sz.tally_words + 1  # the tallies, then the launch's claim counter
 
 
 def test_decode_is_exact_integer_arithmetic():

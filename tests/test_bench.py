@@ -59,3 +59,17 @@ def test_roofline_peaks_say_whether_they_were_measured(tmp_path, monkeypatch):
     assert value == 1651.9 and "measured" in note
     assert bench._peak("hbm_gbs", 1.0) == (6650.0, "hbm_gbs of MEASURED_PEAKS.json (measured)")
     assert bench._peak("sm_max_mhz", 1965.0)[1].startswith("fallback")
+
+
+def test_issue_roofline_of_the_walk_and_the_sweep():
+    """The FP32/SFU issue roofline with the frozen per-step operation counts: skin5 (604.20
+    interaction + 14.30 boundary steps per photon) and the sweep workload (141.1 + 3.8) on 148 SMs
+    at 1965 MHz are SFU-bound at 6.38e8 and 2.73e9 photons/s."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    peak, bound, f_tot, s_tot = bench.issue_roofline(bench.STEPS_PER_PHOTON["skin5"], 148, 1965.0)
+    assert bound == "sfu" and abs(peak / 6.38e8 - 1) < 5e-3
+    assert abs(f_tot - (604.20 * 61 + 14.30 * 25)) < 1e-9 and abs(s_tot - (604.20 * 12 + 14.30 * 3)) < 1e-9
+    peak, bound, _, _ = bench.issue_roofline(bench.SWEEP_STEPS_PER_PHOTON, 148, 1965.0)
+    assert bound == "sfu" and abs(peak / 2.73e9 - 1) < 5e-3

@@ -34,6 +34,7 @@ def test_version():
     (("run", SLAB, "--engine", "tpu"), "--engine must be cuda or b200"),
     (("run", SLAB, "--photons", "-5"), "expects a non-negative integer"),
     (("run", SLAB, "--batches"), "needs a value"),
+    (("run", SLAB, "--step-cap", "0"), "--step-cap must be between 1 and 4294967295"),
 ])
 def test_usage_errors_exit_2(args, needle):
     p = run(*args)
@@ -78,3 +79,17 @@ def test_run_writes_reference_json_layout(tmp_path):
     assert r["engine"] == "cuda" and r["precision"] == "float32" and r["photons"] == 100000
     assert len(r["a_rz"]) == 50 and len(r["a_rz"][0]) == 20 and len(r["rd_ra"][0]) == 30
     assert abs(sum(r["a_z"]) - sum(sum(b["absorbed"]) for b in r["batches"])) < 1e-9 * sum(r["a_z"])
+
+
+@pytest.mark.gpu
+def test_anomalies_make_the_run_exit_1(tmp_path):
+    """A step cap far below a packet's length ends every packet as an anomaly; the command line
+    then exits 1 with the reference's warning (src/cli/main.cpp:162-168) and records them."""
+    out = tmp_path / "r.json"
+    p = run("run", SLAB, "--photons", "20000", "--batches", "4", "--step-cap", "3", "--output", str(out))
+    assert p.returncode == 1, p.stderr
+    assert "anomalies (non-finite weight or non-unit direction)" in p.stderr
+    r = json.loads(out.read_text())["runs"][0]
+    assert r["anomalies"] > 0 and sum(b["anomalies"] for b in r["batches"]) == r["anomalies"]
+    p = run("run", SLAB, "--photons", "20000", "--batches", "4")
+    assert p.returncode == 0, p.stderr

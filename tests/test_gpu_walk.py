@@ -10,14 +10,15 @@ reproducible and independent of the batching.
 from __future__ import annotations
 
 import math
+from pathlib import Path
 
 import numpy as np
 import pytest
 
 import oracle
 import tissuemc_b200 as tmc
-from gates import (batch_estimate, bin_z_scores, compare, conservation, from_engine, from_oracle,
-                   from_reference_json, identical_photon_gaps)
+from gates import (batch_estimate, bin_z_scores, bin_z_two_runs, compare, conservation, family_check, from_engine,
+                   from_oracle, from_reference_json, identical_photon_gaps)
 
 pytestmark = pytest.mark.gpu
 
@@ -124,15 +125,40 @@ def test_profiles_off_diagnostic_keeps_totals(slab):
 def test_run_device_then_decode_equals_run(slab):
     torch = pytest.importorskip("torch")
     opt = tmc.options(photons=30_000, batches=3, seed=4)
-    words = int(tmc.query_sizes(slab, opt).tally_words)
-    buf = torch.empty(words, dtype=torch.int64, device="cuda:0")
+    sz = tmc.query_sizes(slab, opt)
+    buf = torch.empty(int(sz.device_words), dtype=torch.int64, device="cuda:0")
     stream = torch.cuda.current_stream()
     tmc.run_device(slab, opt, buf.data_ptr(), stream.cuda_stream)
     torch.cuda.synchronize()
-    raw = buf.cpu().numpy().view(np.uint64)
+    raw = buf[:int(sz.tally_words)].cpu().numpy().view(np.uint64)
     dec = tmc.decode(slab, opt, raw)
     ref = tmc.run(slab, opt)
     assert np.array_equal(dec.raw, ref.raw)
+
+
+def test_device_runs_on_two_streams_at_once_are_independent(slab):
+    """Two tmc_b200_run_device calls on two streams, with no synchronisation between them (and a
+    tmc_b200_run while they may still be running): each launch claims its photons from a counter in
+    its own buffer, so each buffer holds exactly the tallies of that run alone."""
+    torch = pytest.importorskip("torch")
+    skin = tmc.workload("skin5")
+    jobs = [(slab, tmc.options(photons=400_000, batches=8, seed=1)),
+            (skin, tmc.options(photons=30_000, batches=3, seed=2)),
+            (slab, tmc.options(photons=123_457, batches=5, seed=9))]
+    bufs, streams = [], []
+    for spec, opt in jobs:
+        sz = tmc.query_sizes(spec, opt)
+        bufs.append((torch.full((int(sz.device_words),), -1, dtype=torch.int64, device="cuda:0"), int(sz.tally_words)))
+        streams.append(torch.cuda.Stream(device=0))
+    torch.cuda.synchronize()
+    for (spec, opt), (buf, _), st in zip(jobs, bufs, streams):
+        tmc.run_device(spec, opt, buf.data_ptr(), st.cuda_stream)
+    alone_mid = tmc.run(*jobs[0])  # the regular entry point while the device runs may be in flight
+    torch.cuda.synchronize()
+    for (spec, opt), (buf, words) in zip(jobs, bufs):
+        got = buf[:words].cpu().numpy().view(np.uint64)
+        assert np.array_equal(got, tmc.run(spec, opt).raw)
+    assert np.array_equal(alone_mid.raw, tmc.run(*jobs[0]).raw)
 
 
 # ---------------------------------------------------------------- edge cases and other media
@@ -270,7 +296,109 @@ def test_skin5_vs_float64_engine_independent_seeds(skin):
         assert ok, (key, m, mo, z)
 
 
-# ---------------------------------------------------------------- errors
+# Per-bin parity of the five-layer stack, the workload whose A(r,z) grid (500 x 400) does not fit in
+# shared memory: its deposits go through the shared core tile, the shared "cross" (last row and
+# column) and the global spill, so every routing path of the tally is covered.
+PROFILES_2D = ("a_rz", "rd_ra", "tt_ra")
+
+
+def _gpu_batch_bins(spec: tmc.RunSpec, opt) -> tuple[np.ndarray, dict]:
+    """Per-batch 2-D tallies of one GPU run: each batch of the run's BatchPlan is walked as its own
+    photon-id shard (tmc_b200_run_device_range, the same streams and batch membership as in the
+    whole run) into a buffer of its own, then decoded."""
+    torch = pytest.importorskip("torch")
+    sz = tmc.query_sizes(spec, opt)
+    words, dwords = int(sz.tally_words), int(sz.device_words)
+    sizes = oracle.batch_sizes(int(opt.photons or spec.photons), int(opt.batches))
+    bufs = torch.empty((len(sizes), dwords), dtype=torch.int64, device="cuda:0")
+    stream = torch.cuda.current_stream().cuda_stream
+    first = 0
+    for b, n in enumerate(sizes):
+        tmc.run_device_range(spec, opt, first, int(n), bufs[b].data_ptr(), stream)
+        first += int(n)
+    raw = bufs[:, :words].cpu().numpy().view(np.uint64)
+    del bufs
+    out = {k: np.empty((len(sizes), int(sz.a_rz if k == "a_rz" else sz.ra))) for k in PROFILES_2D}
+    for b in range(len(sizes)):
+        d = tmc.decode(spec, opt, raw[b])
+        for k in PROFILES_2D:
+            out[k][b] = getattr(d, k).ravel()
+    return sizes, out
+
+
+@pytest.fixture(scope="module")
+def skin_f64(skin):
+    """The float64 CPU engine on the five-layer stack: 2e6 photons, 100 batches, seed 7, with per-bin
+    score counts and per-batch 2-D bins."""
+    return oracle.run(_ospec(skin), 2_000_000, 100, 7, 64, threads=0, counts=True, per_batch_bins=True)
+
+
+def _totals_within_3_se(res: tmc.RunResult, o) -> None:
+    pairs = [("rd", res.rd, o.rd), ("tt", res.tt, o.tt)]
+    pairs += [(f"absorbed[{l}]", res.absorbed[:, l], o.absorbed[:, l]) for l in range(o.absorbed.shape[1])]
+    for key, sg, so in pairs:
+        m, se = batch_estimate(sg, res.photons)
+        mo, seo = batch_estimate(so, o.photons)
+        z, ok = compare(m, se, mo, seo)
+        assert ok and abs(z) < 3, (key, m, mo, z)
+
+
+def test_skin5_every_profile_bin_vs_float64_engine_same_photons(skin, skin_f64):
+    """The GPU's float32 walk against the float64 CPU engine on the same 2e6 photons (seed 7, 100
+    batches): |z| < 3 on R_d, T_t, the absorption of every layer, and every A(r,z), R_d(r,a) and
+    T_t(r,a) bin with at least FLOOR contributing scores; each side's standard error from its own
+    per-batch bins."""
+    o = skin_f64
+    opt = tmc.options(photons=2_000_000, batches=100, seed=7)
+    sizes, gpu = _gpu_batch_bins(skin, opt)
+    assert np.array_equal(sizes, o.photons)
+    whole = tmc.run(skin, opt)
+    for k in PROFILES_2D:  # the shards are the run
+        assert np.allclose(gpu[k].sum(axis=0), getattr(whole, k).ravel(), rtol=1e-12, atol=0)
+    _totals_within_3_se(whole, o)
+    tested = {}
+    for k in PROFILES_2D:
+        z, n = bin_z_two_runs(gpu[k], sizes, getattr(o, "b_" + k).reshape(len(o.photons), -1), o.photons,
+                              getattr(o, "n_" + k).ravel(), FLOOR)
+        tested[k] = n
+        assert z.size == 0 or z.max() < 3, (k, float(z.max()), n)
+    assert tested["a_rz"] > 10_000, tested
+    print("skin5 same-photon bins tested:", tested)
+
+
+def test_skin5_profile_bins_vs_an_independent_float64_run(skin, skin_f64):
+    """The GPU at 1e7 photons (seed 101, 100 batches) against the float64 engine's independent 2e6
+    photons (seed 7): totals within |z| < 3, and the |z| of every bin with at least FLOOR scores in the
+    float64 run judged as a family of independent tests (family_check: the count above 3 near its
+    null expectation, the largest below the Bonferroni bound), which a fixed |z| < 3 on each of
+    ~10^4-10^5 independent bins cannot be."""
+    o = skin_f64
+    opt = tmc.options(photons=10_000_000, batches=100, seed=101)
+    sizes, gpu = _gpu_batch_bins(skin, opt)
+    _totals_within_3_se(tmc.run(skin, opt), o)
+    for k in PROFILES_2D:
+        z, n = bin_z_two_runs(gpu[k], sizes, getattr(o, "b_" + k).reshape(len(o.photons), -1), o.photons,
+                              getattr(o, "n_" + k).ravel(), FLOOR)
+        fam = family_check(z, dof=99)
+        print(f"skin5 independent {k}: {fam}")
+        assert fam.passed, (k, str(fam))
+
+
+# ---------------------------------------------------------------- failure paths and errors
+def test_step_cap_turns_endless_packets_into_anomalies(slab):
+    """The per-photon step cap (tmc_options.step_cap) ends a packet that is still alive after that
+    many steps and counts one anomaly for it, instead of looping: with a cap of 3 steps nearly every
+    slab packet (about 20 interactions each) is cut; without a cap none is."""
+    cut = tmc.run(slab, photons=50_000, batches=5, seed=1, step_cap=3)
+    full = tmc.run(slab, photons=50_000, batches=5, seed=1)
+    assert int(full.anomalies.sum()) == 0
+    n_cut = int(cut.anomalies.sum())
+    assert 0.5 * 50_000 < n_cut <= 50_000
+    # a cut packet ran exactly 3 steps: at most 3 absorption events each
+    assert int(cut.events.sum()) <= 3 * 50_000 < int(full.events.sum())
+
+
+
 def test_bad_config_raises_config_error(slab):
     with pytest.raises(tmc.ConfigError, match="batches cannot exceed the number of photons"):
         tmc.run(slab, photons=5, batches=6)
@@ -282,11 +410,11 @@ def test_bad_device_ordinal_is_no_device(slab):
     assert e.value.code == tmc.NO_DEVICE
 
 
-REF_CUDA = oracle.REF_BIN.parent / "tissuemc_cuda"
+REF_CUDA = Path(__file__).resolve().parents[1] / "baseline" / "_ref" / "tissuemc_cuda"
 
 
 @pytest.mark.skipif(not REF_CUDA.exists(),
-                    reason="the reference's CUDA engine is not built here (make -C oracle ref_cuda)")
+                    reason="the reference's CUDA engine is not built here (make -C baseline)")
 @pytest.mark.parametrize("rung", [7, 8])
 def test_slab_identical_photons_vs_the_reference_cuda_engine(slab, slab_gpu, tmp_path, rung):
     """The reference's own GPU engine (its rungs 7 and 8, float32 transport) on the same device,

@@ -75,10 +75,10 @@ def test_int64_allreduce_adds_unsigned_tallies_modulo_2_64():
 def _raw_of_range(spec, opt, first, count):
     import torch
 
-    words = int(tmc.query_sizes(spec, opt).tally_words)
-    d = torch.empty(words, dtype=torch.int64, device="cuda")
+    sz = tmc.query_sizes(spec, opt)
+    d = torch.empty(int(sz.device_words), dtype=torch.int64, device="cuda")
     tmc.run_device_range(spec, opt, first, count, d.data_ptr(), torch.cuda.current_stream().cuda_stream)
-    return d.cpu().numpy().view(np.uint64)
+    return d[:int(sz.tally_words)].cpu().numpy().view(np.uint64)
 
 
 @pytest.mark.gpu
@@ -91,10 +91,11 @@ def test_shards_add_up_to_the_whole_run_bit_for_bit(name, photons, cuts):
     spec = tmc.workload(name)
     spec.photons = photons
     opt = tmc.options(batches=10, seed=3)
-    words = int(tmc.query_sizes(spec, opt).tally_words)
-    whole = torch.empty(words, dtype=torch.int64, device="cuda")
+    sz = tmc.query_sizes(spec, opt)
+    words = int(sz.tally_words)
+    whole = torch.empty(int(sz.device_words), dtype=torch.int64, device="cuda")
     tmc.run_device(spec, opt, whole.data_ptr(), torch.cuda.current_stream().cuda_stream)
-    whole = whole.cpu().numpy().view(np.uint64)
+    whole = whole[:words].cpu().numpy().view(np.uint64)
     bounds = [0, *cuts, photons]
     total = np.zeros(words, np.uint64)
     with np.errstate(over="ignore"):

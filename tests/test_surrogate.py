@@ -58,6 +58,24 @@ def test_gemm_rejects_k_not_multiple_of_64():
         tmc.gemm_bf16(A, A)
 
 
+def test_a_wait_that_runs_out_reports_device_timeout_and_leaves_the_device_usable():
+    """The GEMM kernel's producer is told to issue no loads, so the MMA issuer's bounded wait (4096
+    polls) runs out with nothing outstanding: the kernel skips its epilogue, frees its tensor memory
+    and raises its status word, which the host turns into TMC_DEVICE_TIMEOUT. A normal product on
+    the same device afterwards is still exact."""
+    rc, msg = tmc.probe_wait_timeout(4096)
+    assert rc == tmc.DEVICE_TIMEOUT, (rc, msg)
+    assert "gave up" in msg
+    rc, msg = tmc.probe_wait_timeout(4096)  # and again: the status word was cleared
+    assert rc == tmc.DEVICE_TIMEOUT, (rc, msg)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    A = torch.randn(256, 128, device="cuda", generator=g).bfloat16()
+    B = torch.randn(192, 128, device="cuda", generator=g).bfloat16()
+    D = tmc.gemm_bf16(A, B)
+    ref = A.double() @ B.double().T
+    assert ((D.double() - ref).abs().max() / ref.abs().max()).item() < 2e-6
+
+
 def _member_numpy(m):
     Ws = [bf16(w.cpu().numpy()) for w in m.W]
     bs = [b.cpu().numpy().astype(np.float64) for b in m.b]

@@ -1,9 +1,8 @@
 """The allocation-free entry point, tmc_b200_run_static.
 
-It serves callers that cannot call cudaMalloc — a host program running while a stream is being
-captured into a CUDA graph, or a framework that owns all device memory through its own pool — by
-keeping the walk's scratch (claim counter and fixed-point tallies) in a static device array of the
-library. These tests call it through the C ABI and hold it to the regular entry point,
+It serves callers that cannot call cudaMalloc — a framework that owns all device memory through
+its own pool, or a plugin host that gives each plugin a fixed memory budget — by keeping the walk's
+scratch (claim counter and fixed-point tallies) in a static device array of the library. These tests call it through the C ABI and hold it to the regular entry point,
 tmc_b200_run, bit for bit (integer tallies: the tolerance is zero), on consecutive calls that
 reuse the same array. This file is collected last on purpose.
 """
@@ -11,6 +10,11 @@ reuse the same array. This file is collected last on purpose.
 from __future__ import annotations
 
 import ctypes
+import json
+import subprocess
+import sys
+import textwrap
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -67,3 +71,38 @@ def test_static_entry_point_needs_the_raw_buffer():
     st = tmc.CStatus()
     rc = lib.tmc_b200_run_static(ctypes.byref(spec), ctypes.byref(opt), ctypes.byref(res), ctypes.byref(st))
     assert rc == tmc.BAD_ARGUMENT and b"raw" in st.message
+
+
+# Run in a fresh process, so that nothing else has set the device up: the allocation-free entry
+# point is called first and alone, and the device's free memory must not move across later calls.
+_FRESH = textwrap.dedent("""
+    import json, sys
+    sys.path.insert(0, sys.argv[1])
+    import numpy as np
+    import torch
+    import tissuemc_b200 as tmc
+
+    slab = tmc.workload("slab_n14")
+    opt = tmc.options(photons=200_000, batches=20, seed=3)
+    first = tmc.run_static(slab, opt)                   # sets the device up
+    free_after_first = torch.cuda.mem_get_info(0)[0]
+    second = tmc.run_static(slab, opt)
+    third = tmc.run_static(slab, opt)
+    free_after_third = torch.cuda.mem_get_info(0)[0]
+    ref = tmc.run(slab, opt)                            # the regular entry point, which allocates
+    same = all(np.array_equal(getattr(a, f), getattr(ref, f))
+               for a in (first, second, third) for f in ("raw", "rd", "tt", "absorbed", "events", "a_rz"))
+    print(json.dumps({"free_after_first": free_after_first, "free_after_third": free_after_third,
+                      "same": same, "device": torch.cuda.current_device()}))
+""")
+
+
+@pytest.mark.gpu
+def test_static_entry_point_allocates_nothing_in_a_fresh_process():
+    root = Path(__file__).resolve().parents[1]
+    p = subprocess.run([sys.executable, "-c", _FRESH, str(root)], capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    out = json.loads(p.stdout.strip().splitlines()[-1])
+    assert out["same"]
+    assert out["free_after_first"] == out["free_after_third"], out
+    assert out["device"] == 0

@@ -75,12 +75,13 @@ class COptions(ctypes.Structure):
         ("threads_per_block", ctypes.c_int32),
         ("blocks_per_sm", ctypes.c_int32),
         ("smem_budget", ctypes.c_int32),
+        ("step_cap", ctypes.c_uint32),
     ]
 
 
 class CSizes(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in
-                ("batches", "layers", "nz", "nr", "na", "absorbed", "a_rz", "ra", "tally_words")]
+                ("batches", "layers", "nz", "nr", "na", "absorbed", "a_rz", "ra", "tally_words", "device_words")]
 
 
 _pd, _pu = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)
@@ -169,6 +170,7 @@ PROTOTYPES = {
                                                _P(CStatus)]),
     "tmc_b200_sweep_autotune": (ctypes.c_int, [_P(CSweepConfig), ctypes.c_int32, _P(CSweepOptions), _pd,
                                                _P(CStatus)]),
+    "tmc_b200_probe_wait_timeout": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint32, _P(CStatus)]),
     "tmc_b200_gemm_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
                                           _P(CStatus)]),
@@ -285,12 +287,13 @@ class RunSpec:
 
 def options(seed: int = 1, batches: int = 10, photons: int = 0, rung: int = 0, profiles: bool = True,
             device: int = 0, fast_math: bool = True, threads_per_block: int = 0, blocks_per_sm: int = 0,
-            smem_budget: int = 0) -> COptions:
+            smem_budget: int = 0, step_cap: int = 0) -> COptions:
     o = COptions()
     lib().tmc_b200_default_options(ctypes.byref(o))
     o.seed, o.batches, o.photons, o.rung = seed, batches, photons, rung
     o.profiles, o.device, o.fast_math = int(profiles), device, int(fast_math)
     o.threads_per_block, o.blocks_per_sm, o.smem_budget = threads_per_block, blocks_per_sm, smem_budget
+    o.step_cap = step_cap
     return o
 
 
@@ -456,7 +459,8 @@ def decode(spec: RunSpec, opt: COptions, raw: np.ndarray) -> RunResult:
 
 
 def run_device(spec: RunSpec, opt: COptions, d_tally_ptr: int, stream_ptr: int = 0) -> None:
-    """Launch the walk into a device tally buffer on a stream, without synchronising."""
+    """Launch the walk into a device buffer of query_sizes(...).device_words words (the tallies,
+    then the launch's claim counter) on a stream, without synchronising."""
     st = CStatus()
     c = spec.to_c()
     _check(lib().tmc_b200_run_device(ctypes.byref(c), ctypes.byref(opt), ctypes.c_void_p(d_tally_ptr),
@@ -465,13 +469,22 @@ def run_device(spec: RunSpec, opt: COptions, d_tally_ptr: int, stream_ptr: int =
 
 def run_device_range(spec: RunSpec, opt: COptions, first_photon: int, count: int, d_tally_ptr: int,
                      stream_ptr: int = 0) -> None:
-    """Launch one shard of a run (photons [first_photon, first_photon + count)) into a device tally
-    buffer on a stream, without synchronising; the shards of a partition add up to the run."""
+    """Launch one shard of a run (photons [first_photon, first_photon + count)) into a device buffer
+    of device_words words on a stream, without synchronising; the shards of a partition add up to
+    the run (their first tally_words words)."""
     st = CStatus()
     c = spec.to_c()
     _check(lib().tmc_b200_run_device_range(ctypes.byref(c), ctypes.byref(opt), first_photon, count,
                                            ctypes.c_void_p(d_tally_ptr), ctypes.c_void_p(stream_ptr),
                                            ctypes.byref(st)), st)
+
+
+def probe_wait_timeout(wait_limit: int = 4096, device: int = 0) -> tuple[int, str]:
+    """Make the tensor-core GEMM kernel's bounded wait run out on purpose (its producer issues no
+    loads) and return (status code, message): DEVICE_TIMEOUT when the kernel reported the give-up."""
+    st = CStatus()
+    rc = lib().tmc_b200_probe_wait_timeout(device, wait_limit, ctypes.byref(st))
+    return rc, st.message.decode(errors="replace")
 
 
 def probe_physics(what: str, g: float, mu_t: float = 10.0, samples: int = 1_000_000, seed: int = 7,

@@ -251,7 +251,7 @@ WalkParams make_params(const tmc_run_spec &spec, const tmc_options &opt, const P
     P.cross = pl.cross;
     P.batch_smem = pl.batch_smem;
     P.profiles = opt.profiles ? 1 : 0;
-    P.step_cap = 2000000000u;
+    P.step_cap = opt.step_cap ? opt.step_cap : kDefaultStepCap;
     // ids a warp claims at once: one per lane, so that when the ids run out no warp is left holding
     // a backlog of unstarted photons while others idle
     P.chunk = 32;
@@ -268,12 +268,13 @@ WalkParams make_params(const tmc_run_spec &spec, const tmc_options &opt, const P
 
 namespace {
 
-// Launch the walk on `stream` into `d_tally` (zeroed here). Records ev0/ev1 around it if given.
+// Launch the walk on `stream` into `d_tally` (zeroed here), claiming photon ids from `counter`
+// (zeroed here; a word no other launch in flight uses). Records ev0/ev1 around it if given.
 // With count > 0, only photons [first, first + count) of the run are walked (a shard: the same
 // streams and batches as in the whole run, so the shards' tallies add up to the run's).
 void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
-                 unsigned long long *d_tally, cudaStream_t stream, cudaEvent_t e0, cudaEvent_t e1,
-                 uint64_t first = 0, uint64_t count = 0) {
+                 unsigned long long *d_tally, unsigned long long *counter, cudaStream_t stream, cudaEvent_t e0,
+                 cudaEvent_t e1, uint64_t first = 0, uint64_t count = 0) {
     const RunShape sh = shape_of(spec, opt);
     const size_t words = tally_offsets(sh).total;
     int regs_bps = 0;
@@ -283,7 +284,7 @@ void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
     else
         TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&regs_bps, walk_kernel<0>, threads, 0));
     const Plan pl = make_plan(spec, opt, limits_of(c.prop), regs_bps);
-    WalkParams P = make_params(spec, opt, pl, d_tally, reinterpret_cast<unsigned int *>(c.d_counter));
+    WalkParams P = make_params(spec, opt, pl, d_tally, reinterpret_cast<unsigned int *>(counter));
     if (count) {
         P.photons = count;
         P.id_base = static_cast<uint32_t>(first);
@@ -296,7 +297,7 @@ void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
     const int grid = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(pl.grid), max_blocks));
     if (e0) TMC_CUDA(cudaEventRecord(e0, stream));
     TMC_CUDA(cudaMemsetAsync(d_tally, 0, words * 8, stream));
-    TMC_CUDA(cudaMemsetAsync(c.d_counter, 0, 8, stream));
+    TMC_CUDA(cudaMemsetAsync(counter, 0, 8, stream));
     if (opt.fast_math)
         walk_kernel<1><<<grid, pl.threads, smem, stream>>>(P);
     else
@@ -315,7 +316,8 @@ double run_single_loop(const tmc_run_spec *specs, const tmc_options *opts, int n
     DeviceCtx &c = device_ctx(opts[0].device);
     ensure_tally(c, off[n]);
     TMC_CUDA(cudaEventRecord(c.ev0, c.stream));
-    for (int i = 0; i < n; ++i) launch_walk(specs[i], opts[i], c, c.d_tally + off[i], c.stream, nullptr, nullptr);
+    for (int i = 0; i < n; ++i)
+        launch_walk(specs[i], opts[i], c, c.d_tally + off[i], c.d_counter, c.stream, nullptr, nullptr);
     TMC_CUDA(cudaEventRecord(c.ev1, c.stream));
     TMC_CUDA(cudaStreamSynchronize(c.stream));
     float ms = 0.f;
@@ -328,13 +330,27 @@ double run_single_loop(const tmc_run_spec *specs, const tmc_options *opts, int n
     return static_cast<double>(ms) / 1000.0;
 }
 // ------------------------------------------------------------- allocation-free entry point
-// Some callers cannot allocate device memory: a host program that runs while a CUDA stream is
-// being captured into a graph (cudaMalloc is not permitted during capture), or a framework that
-// owns every byte of device memory through its own pool and forbids libraries from calling
-// cudaMalloc. tmc_b200_run_static serves them: the walk's scratch (its photon-claim counter and
-// the fixed-point tally accumulators) lives in the file-scope array below, which the CUDA
-// runtime places in every device's memory when the library is loaded and keeps until exit.
+// Some callers cannot allocate device memory: a framework that owns every byte of device memory
+// through its own pool and forbids libraries from calling cudaMalloc, or a plugin host that gives
+// each plugin a fixed memory budget. tmc_b200_run_static serves them: the walk's scratch (its
+// photon-claim counter and the fixed-point tally accumulators) lives in the file-scope array
+// below, which the CUDA runtime places in every device's memory when the library's module is
+// loaded there and keeps until exit.
 namespace {
+
+// Restores the calling thread's current device when the call returns (every exit path).
+struct DeviceGuard {
+    int saved = -1;
+    DeviceGuard() {
+        if (cudaGetDevice(&saved) != cudaSuccess) {
+            cudaGetLastError();
+            saved = -1;
+        }
+    }
+    ~DeviceGuard() {
+        if (saved >= 0) cudaSetDevice(saved);
+    }
+};
 
 constexpr size_t kStaticHeadWords = 32;  // word 0: claim counter; the tallies start 256 B in
 __device__ __align__(256) unsigned long long g_static_scratch[kStaticHeadWords + TMC_B200_STATIC_SCRATCH_WORDS];
@@ -406,7 +422,7 @@ int tmc_b200_run(const tmc_run_spec *spec, const tmc_options *opt, tmc_result *r
         DeviceCtx &c = device_ctx(opt->device);
         ensure_tally(c, words);
         ensure_stage(c, words);
-        launch_walk(*spec, *opt, c, c.d_tally, c.stream, c.ev0, c.ev1);
+        launch_walk(*spec, *opt, c, c.d_tally, c.d_counter, c.stream, c.ev0, c.ev1);
         TMC_CUDA(cudaMemcpyAsync(c.h_stage, c.d_tally, words * 8, cudaMemcpyDeviceToHost, c.stream));
         TMC_CUDA(cudaStreamSynchronize(c.stream));
         float ms = 0.f;
@@ -446,8 +462,10 @@ int tmc_b200_run_device_range(const tmc_run_spec *spec, const tmc_options *opt, 
                                 std::to_string(first_photon + count) + ") is empty or beyond the run's " +
                                 std::to_string(total) + " photons");
         DeviceCtx &c = device_ctx(opt->device);
-        launch_walk(*spec, *opt, c, reinterpret_cast<unsigned long long *>(d_tally),
-                    static_cast<cudaStream_t>(stream), nullptr, nullptr, first_photon, count);
+        unsigned long long *tally = reinterpret_cast<unsigned long long *>(d_tally);
+        const size_t words = tally_offsets(shape_of(*spec, *opt)).total;
+        launch_walk(*spec, *opt, c, tally, tally + words, static_cast<cudaStream_t>(stream), nullptr, nullptr,
+                    first_photon, count);
         return TMC_OK;
     } catch (const ConfigFailure &e) {
         set_status(st, TMC_BAD_CONFIG, e.what());
@@ -472,8 +490,9 @@ int tmc_b200_run_device(const tmc_run_spec *spec, const tmc_options *opt, uint64
     try {
         validate_run(*spec, *opt);
         DeviceCtx &c = device_ctx(opt->device);
-        launch_walk(*spec, *opt, c, reinterpret_cast<unsigned long long *>(d_tally),
-                    static_cast<cudaStream_t>(stream), nullptr, nullptr);
+        unsigned long long *tally = reinterpret_cast<unsigned long long *>(d_tally);
+        const size_t words = tally_offsets(shape_of(*spec, *opt)).total;
+        launch_walk(*spec, *opt, c, tally, tally + words, static_cast<cudaStream_t>(stream), nullptr, nullptr);
         return TMC_OK;
     } catch (const ConfigFailure &e) {
         set_status(st, TMC_BAD_CONFIG, e.what());
@@ -499,6 +518,7 @@ int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_re
         validate_run(*spec, *opt);
         const RunShape sh = shape_of(*spec, *opt);
         const size_t words = tally_offsets(sh).total;
+        const DeviceGuard keep_device;
         if (words > TMC_B200_STATIC_SCRATCH_WORDS) {
             throw Fail(TMC_BAD_CONFIG,
                        "this run needs " + std::to_string(words) + " tally words but the static scratch of "
@@ -529,8 +549,9 @@ int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_re
         else
             walk_kernel<0><<<grid, pl.threads, smem, 0>>>(P);
         TMC_CUDA(cudaGetLastError());
-        TMC_CUDA(cudaMemcpy(res->raw, tally, words * 8, cudaMemcpyDeviceToHost));
+        TMC_CUDA(cudaStreamSynchronize(0));
         const auto k1 = std::chrono::steady_clock::now();
+        TMC_CUDA(cudaMemcpy(res->raw, tally, words * 8, cudaMemcpyDeviceToHost));
         uint64_t *raw = res->raw;
         res->raw = nullptr;  // decode into the other arrays without copying raw onto itself
         decode_tallies(*spec, *opt, raw, *res);

@@ -10,8 +10,14 @@
 //   issuer) waits for a stage, issues its four tcgen05.mma (K = 16 each) into the TMEM accumulator
 //   and commits them to the stage's "empty" mbarrier, which hands the stage back to the producer;
 //   a last commit marks the accumulator complete. Rows past M or N arrive as zeros. Every wait is
-//   bounded: one that runs out records an error in *status (the host discards the results), and
-//   the producer waits (bounded) for every load it issued before the CTA may exit.
+//   bounded: one that runs out records an error in *status (the host discards the results) and
+//   the CTA skips its epilogue. Nothing is released while this CTA's own asynchronous work may
+//   still be in flight: the issuer commits the accumulator barrier after whatever MMAs it issued
+//   (also when it gave up), every warp waits for that barrier before TMEM is read or freed, and
+//   the producer waits for every load it issued; these drain waits have a longer limit of their
+//   own (issued copies and MMAs finish without help from any other party). Only if a drain wait
+//   runs out too does the CTA free TMEM regardless (so that a later CTA can allocate it) and
+//   report status 2.
 //   The epilogue reads the accumulator with tcgen05.ld, 32 columns per load (warp w owns TMEM
 //   lanes 32w..32w+31, i.e. output rows m0 + 32w + lane), applies the epilogue functor (given the
 //   split index) to each 8 columns and writes global memory.
@@ -25,22 +31,28 @@
 namespace tmc {
 
 constexpr int kGemmBM = 128, kGemmBK = 64, kGemmThreads = 128, kGemmStages = 3;
-constexpr uint32_t kGemmWaitLimit = 1u << 24;  // mbarrier polls before a wait gives up
+constexpr uint32_t kGemmWaitLimit = 1u << 24;   // mbarrier polls before a wait gives up
+constexpr uint32_t kGemmDrainLimit = 1u << 26;  // polls of a wait for this CTA's own issued work
 
 template <int BN> struct GemmSmem {
     static constexpr int a_bytes = kGemmBM * 128;  // 128 rows x 64 bf16
     static constexpr int b_bytes = BN * 128;
     static constexpr int stage_bytes = a_bytes + b_bytes;
-    // alignment slack, the stages, then 2 x kGemmStages + 1 mbarriers and the TMEM address
+    // alignment slack, the stages, then 2 x kGemmStages + 1 mbarriers, the TMEM address and the
+    // CTA's abort flag
     static constexpr int bytes = 1024 + kGemmStages * stage_bytes + 128;
 };
 
 // Epilogue functor interface: operator()(split, row, col0, v[8]) for 8 consecutive columns of one
 // row (col0 is a multiple of 8; columns at or beyond N must be ignored by the functor).
+// wait_limit bounds the waits on the other roles (kGemmWaitLimit in production). withhold = 1 is
+// a test of the give-up path: the producer issues no loads, so the issuer's first wait runs out
+// with no copy and no MMA outstanding.
 template <int BN, class Epi>
 __global__ void __launch_bounds__(kGemmThreads) gemm_tc_kernel(const __grid_constant__ CUtensorMap tma_a,
                                                               const __grid_constant__ CUtensorMap tma_b, int M, int N,
-                                                              int K, Epi epi, int *status) {
+                                                              int K, Epi epi, int *status, uint32_t wait_limit,
+                                                              int withhold) {
     static_assert(GemmSmem<BN>::a_bytes % 1024 == 0 && GemmSmem<BN>::b_bytes % 1024 == 0, "1024-byte tiles");
     extern __shared__ unsigned char gsm_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
@@ -49,6 +61,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_tc_kernel(const __grid_cons
     uint64_t *empty = full + kGemmStages;
     uint64_t *acc_bar = empty + kGemmStages;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_bar + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * kGemmBM, n0 = blockIdx.x * BN;
@@ -59,6 +72,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_tc_kernel(const __grid_cons
             mbar_init(&empty[s], 1);
         }
         mbar_init(acc_bar, 1);
+        *abort_flag = 0;
     }
     tc_fence_before();
     __syncthreads();
@@ -72,11 +86,11 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_tc_kernel(const __grid_cons
     if (warp == 0) {
         // ---- producer: the whole warp walks the ring, lane 0 issues
         int issued = 0;
-        for (int kt = 0; kt < kt_n; ++kt) {
+        for (int kt = 0; kt < (withhold ? 0 : kt_n); ++kt) {
             const int s = kt % kGemmStages;
             // the stage was last read by the MMAs of slice kt - kGemmStages
             if (kt >= kGemmStages &&
-                !mbar_wait(&empty[s], static_cast<uint32_t>((kt / kGemmStages - 1) & 1), kGemmWaitLimit)) {
+                !mbar_wait(&empty[s], static_cast<uint32_t>((kt / kGemmStages - 1) & 1), wait_limit)) {
                 ok = false;
                 break;
             }
@@ -91,13 +105,15 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_tc_kernel(const __grid_cons
         }
         // every load issued has landed before the CTA can end (the last phase of each stage)
         for (int kt = issued > kGemmStages ? issued - kGemmStages : 0; kt < issued; ++kt)
-            if (!mbar_wait(&full[kt % kGemmStages], static_cast<uint32_t>((kt / kGemmStages) & 1), kGemmWaitLimit))
+            if (!mbar_wait(&full[kt % kGemmStages], static_cast<uint32_t>((kt / kGemmStages) & 1), kGemmDrainLimit)) {
                 ok = false;
+                if (lane == 0) atomicExch(status, 2);
+            }
     } else if (warp == 1) {
         // ---- issuer: the whole warp waits, lane 0 issues the MMAs and the commits
         for (int kt = 0; kt < kt_n; ++kt) {
             const int s = kt % kGemmStages;
-            if (!mbar_wait(&full[s], static_cast<uint32_t>((kt / kGemmStages) & 1), kGemmWaitLimit)) {
+            if (!mbar_wait(&full[s], static_cast<uint32_t>((kt / kGemmStages) & 1), wait_limit)) {
                 ok = false;
                 break;
             }
@@ -113,16 +129,23 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_tc_kernel(const __grid_cons
             }
             __syncwarp();
         }
-        if (lane == 0) umma_commit(acc_bar);  // arrives when every MMA issued above has completed
+        // arrives when every MMA issued above has completed, also after a give-up
+        if (lane == 0) umma_commit(acc_bar);
         __syncwarp();
     }
-    if (!ok && lane == 0) atomicExch(status, 1);
-    if (ok && !mbar_wait(acc_bar, 0u, kGemmWaitLimit)) {
-        ok = false;
-        atomicExch(status, 1);
+    if (!ok) {
+        if (lane == 0) atomicCAS(status, 0, 1);
+        *abort_flag = 1;
+    }
+    // every MMA this CTA issued has completed before TMEM is read or released
+    if (!mbar_wait(acc_bar, 0u, wait_limit)) {
+        if (lane == 0) atomicCAS(status, 0, 1);
+        *abort_flag = 1;
+        if (!mbar_wait(acc_bar, 0u, kGemmDrainLimit) && lane == 0) atomicExch(status, 2);
     }
     tc_fence_after();
-    ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld is warp-collective
+    __syncthreads();                 // orders the abort flag: the epilogue runs in every warp or none
+    ok = *abort_flag == 0;
     if (ok) {
         const int row = m0 + warp * 32 + lane;
         const uint32_t lane_addr = tmem_d + (static_cast<uint32_t>(warp * 32) << 16);

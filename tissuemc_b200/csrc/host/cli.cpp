@@ -4,7 +4,7 @@
 //   tissuemc --version
 //   tissuemc run <input.mci> [--photons N] [--batches B] [--seed S] [--threads T] [--precision P]
 //                            [--engine cuda|b200] [--rung N] [--gpu-tally P] [--no-profiles]
-//                            [--output FILE] [--mco FILE]
+//                            [--output FILE] [--mco FILE] [--step-cap N]
 //
 // --engine defaults to the GPU here: this binary carries the B200 engine only (the reference's CPU
 // engine stays the reference's). --threads and --precision are accepted and recorded as the
@@ -18,6 +18,7 @@
 #include <string>
 
 #include "../../../include/tissuemc_b200.h"
+#include "b200_options.hpp"
 #include "tissuemc_api.hpp"
 
 namespace {
@@ -40,7 +41,9 @@ void usage(std::FILE *to) {
                  "  --no-profiles  diagnostic for rung 6: skip the profile tallies\n"
                  "  --output FILE  write full results as JSON\n"
                  "  --mco FILE     also write each run as an MCML output file (FILE, or FILE's stem\n"
-                 "                 with _<run> appended when the input holds several runs)\n");
+                 "                 with _<run> appended when the input holds several runs)\n"
+                 "  --step-cap N   end a packet still alive after N steps and count it as an\n"
+                 "                 anomaly (default 2000000000)\n");
 }
 
 unsigned long long count_arg(const char *name, const char *text) {
@@ -159,6 +162,13 @@ int run_command(int argc, char **argv) {
             output = value("--output");
         } else if (a == "--mco") {
             mco = value("--mco");
+        } else if (a == "--step-cap") {
+            const uint64_t cap = count_arg("--step-cap", value("--step-cap"));
+            if (cap == 0 || cap > 0xFFFFFFFFull) {
+                std::fprintf(stderr, "tissuemc: --step-cap must be between 1 and 4294967295\n");
+                return 2;
+            }
+            tissuemc_b200::set_step_cap(static_cast<uint32_t>(cap));
         } else {
             std::fprintf(stderr, "tissuemc: unknown option '%s'\n", a.c_str());
             usage(stderr);

@@ -165,6 +165,7 @@ int tmc_b200_query_sizes(const tmc_run_spec *spec, const tmc_options *opt, tmc_s
     sz->a_rz = sz->nr * sz->nz;
     sz->ra = sz->nr * sz->na;
     sz->tally_words = tally_offsets(sh).total;
+    sz->device_words = sz->tally_words + 1;  // + the launch's photon-claim counter
     return TMC_OK;
 }
 

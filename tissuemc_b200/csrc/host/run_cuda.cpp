@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../../include/tissuemc_b200.h"
+#include "b200_options.hpp"
 #ifdef TISSUEMC_B200_REFERENCE_HEADERS
 // Built inside TissueMC in place of src/cuda/engine.cu: its own headers declare the interface.
 #include "tissuemc/config.hpp"
@@ -19,6 +20,17 @@
 #else
 #include "tissuemc_api.hpp"
 #endif
+
+namespace tissuemc_b200 {
+
+namespace {
+uint32_t g_step_cap = 0;
+}
+
+void set_step_cap(uint32_t cap) { g_step_cap = cap; }
+uint32_t step_cap() { return g_step_cap; }
+
+}  // namespace tissuemc_b200
 
 namespace tissuemc {
 
@@ -52,6 +64,7 @@ tmc_options to_c(const EngineOptions &o) {
     c.photons = o.photons;
     c.rung = o.rung;
     c.profiles = o.profiles ? 1 : 0;
+    c.step_cap = tissuemc_b200::step_cap();
     return c;
 }
 

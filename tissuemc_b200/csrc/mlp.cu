@@ -394,7 +394,7 @@ bool encode_operand(CUtensorMap *map, const void *ptr, int rows, int K, int box_
 // Common checks and the launch of one tensor-core GEMM (asynchronous).
 template <class Epi>
 int launch_gemm(const void *A, const void *B, int M, int N, int K, const Epi &epi, void *stream, tmc_status *st,
-                int splits = 1) {
+                int splits = 1, uint32_t wait_limit = kGemmWaitLimit, int withhold = 0) {
     if (!A || !B) {
         put(st, TMC_BAD_ARGUMENT, "NULL argument");
         return TMC_BAD_ARGUMENT;
@@ -443,7 +443,7 @@ int launch_gemm(const void *A, const void *B, int M, int N, int K, const Epi &ep
     }
     const dim3 grid((N + kBN - 1) / kBN, (M + kGemmBM - 1) / kGemmBM, splits);
     gemm_tc_kernel<kBN, Epi><<<grid, kGemmThreads, kGemmSmemRequest, static_cast<cudaStream_t>(stream)>>>(
-        ta, tb, M, N, K, epi, status);
+        ta, tb, M, N, K, epi, status, wait_limit, withhold);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         put(st, TMC_CUDA_ERROR, std::string("CUDA error launching the tensor-core GEMM: ") + cudaGetErrorString(e));
@@ -501,6 +501,65 @@ int tmc_b200_gemm_bf16(const uint16_t *A, const uint16_t *B, const float *bias, 
         return TMC_DEVICE_TIMEOUT;
     }
     return TMC_OK;
+}
+
+int tmc_b200_probe_wait_timeout(int32_t device, uint32_t wait_limit, tmc_status *st) {
+    put(st, TMC_OK, "");
+    if (wait_limit < 1 || wait_limit > kGemmWaitLimit) {
+        put(st, TMC_BAD_ARGUMENT, "wait_limit must be between 1 and the production limit");
+        return TMC_BAD_ARGUMENT;
+    }
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        put(st, TMC_NO_DEVICE, "no usable CUDA device found");
+        return TMC_NO_DEVICE;
+    }
+    int saved = 0;
+    cudaGetDevice(&saved);
+    cudaSetDevice(device);
+    // one 128 x 128 x 64 product whose producer issues no loads: the issuer's wait runs out
+    void *buf = nullptr;
+    const size_t a_bytes = 128 * 64 * 2, d_bytes = 128 * 128 * 4;
+    if (cudaMalloc(&buf, 2 * a_bytes + d_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        cudaSetDevice(saved);
+        put(st, TMC_CUDA_ERROR, "CUDA error: cannot allocate the probe's operands");
+        return TMC_CUDA_ERROR;
+    }
+    cudaMemset(buf, 0, 2 * a_bytes + d_bytes);
+    unsigned char *b = static_cast<unsigned char *>(buf);
+    int *status = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        status = status_word(device);
+    }
+    int rc = TMC_OK;
+    if (!status) {
+        put(st, TMC_NO_DEVICE, "no usable CUDA device found");
+        rc = TMC_NO_DEVICE;
+    } else {
+        cudaMemset(status, 0, sizeof(int));
+        rc = launch_gemm(b, b + a_bytes, 128, 128, 64, EpiF32{reinterpret_cast<float *>(b + 2 * a_bytes), nullptr, 128, 0},
+                         nullptr, st, 1, wait_limit, 1);
+        if (rc == TMC_OK) {
+            const cudaError_t e = cudaDeviceSynchronize();
+            int h = 0;
+            if (e == cudaSuccess) cudaMemcpy(&h, status, sizeof(int), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) {
+                put(st, TMC_CUDA_ERROR, std::string("CUDA error in the wait probe: ") + cudaGetErrorString(e));
+                rc = TMC_CUDA_ERROR;
+            } else if (h) {
+                put(st, TMC_DEVICE_TIMEOUT, h == 1 ? "a tensor-core wait gave up (mbarrier poll limit)"
+                                                   : "a tensor-core wait gave up and the CTA's own work did not drain");
+                rc = TMC_DEVICE_TIMEOUT;
+            }
+            cudaMemset(status, 0, sizeof(int));
+        }
+    }
+    cudaFree(buf);
+    cudaSetDevice(saved);
+    return rc;
 }
 
 int tmc_b200_nn_linear(const uint16_t *X, const uint16_t *W, const float *bias, float *Z, uint16_t *H, uint16_t *HT,

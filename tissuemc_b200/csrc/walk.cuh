@@ -24,6 +24,7 @@ namespace tmc {
 
 constexpr int kMaxLayers = 16;
 constexpr float kFixedScale = 4294967296.0f;  // 2^32
+constexpr uint32_t kDefaultStepCap = 2000000000u;  // steps after which a live packet is an anomaly
 
 // Constants of one layer, computed on the host in float arithmetic in the same order as the
 // reference evaluates them (so e.g. hg_a is exactly float(1) - g * g).
