@@ -90,6 +90,14 @@ typedef struct {
     uint32_t step_cap;         /* a packet still alive after this many steps is ended and counted
                                   as an anomaly (0 = 2,000,000,000); no reference counterpart: the
                                   reference loops until the packet dies (physics.hpp:279-287) */
+    /* Shared-memory tally tiles, for grids whose tallies do not all fit (tmc_b200_plan,
+     * tmc_b200_autotune); they change where deposits are summed, never the results. */
+    int32_t tile_tz;           /* depth bins of the shared core tile of A(r,z); its radial rows
+                                  follow from the budget. 0 = planner (about 2 sqrt(tile words)) */
+    int32_t tile_ra_rows;      /* radial rows of R_d(r,a) and of T_t(r,a) kept in shared memory:
+                                  0 = planner (an eighth of the budget each), -1 = none */
+    int32_t tile_cross;        /* the clamped last row and last column of A(r,z) in shared memory:
+                                  0 or 1 = when they fit (planner), -1 = never */
 } tmc_options;
 
 /* Element counts of every output buffer for a run (tmc_b200_query_sizes). */
@@ -190,6 +198,19 @@ typedef struct {
 TMC_B200_API int tmc_b200_plan(const tmc_run_spec *spec, const tmc_options *opt, int32_t sms, int64_t smem_per_sm,
                   int64_t smem_per_block_optin, int64_t reserved_per_block, int32_t regs_blocks_per_sm,
                   tmc_plan *plan, tmc_status *status);
+
+/* Autotune the walk's launch and tally-tile plan for this run on its device: time candidate plans
+ * (blocks per SM, block size, the shared A(r,z) core tile's shape, the shared rows of R_d(r,a) and
+ * T_t(r,a), the shared "cross" of A(r,z)) by coordinate descent on a sample of the run
+ * (min(photons, sample_photons) photons, the run's seed and batches), each the best of two timed
+ * launches after one warm-up, and write the fastest into opt's threads_per_block, blocks_per_sm,
+ * tile_tz, tile_ra_rows and tile_cross. The results of a run do not depend on the plan (integer
+ * tallies). plan (optional) receives the chosen plan; default_seconds and best_seconds (optional)
+ * the sample's kernel time with the planner's default plan and with the chosen one. Replaces the
+ * fixed occupancy sizing of the reference's GPU engine (src/cuda/engine.cu:216-239). */
+TMC_B200_API int tmc_b200_autotune(const tmc_run_spec *spec, tmc_options *opt, uint64_t sample_photons,
+                                   tmc_plan *plan, double *default_seconds, double *best_seconds,
+                                   tmc_status *status);
 
 /* Capacity of the static scratch used by tmc_b200_run_static, in 64-bit tally words (512 KiB). */
 #define TMC_B200_STATIC_SCRATCH_WORDS 65536u

@@ -138,6 +138,35 @@ def test_plan_fits_whole_grids_and_tiles_big_ones():
     assert p.smem_bytes <= max(4096, ring + 5 * 96) + 16 and p.cross == 0 and p.tr_a == 0
 
 
+def test_plan_follows_the_tile_options():
+    """The tile options the autotuner searches: the core tile's depth, the shared rows of R_d(r,a) and
+    T_t(r,a), and the cross; every combination stays within the per-block budget."""
+    skin = tmc.workload("skin5")
+    base = tmc.plan(skin, tmc.options(batches=100))
+    p = tmc.plan(skin, tmc.options(batches=100, tile_tz=40))
+    assert p.tz_a == 40 and p.tr_a > base.tr_a and p.cross == 1
+    p = tmc.plan(skin, tmc.options(batches=100, tile_tz=4000))  # clamped: the cross holds the last column
+    assert p.tz_a == 399
+    p = tmc.plan(skin, tmc.options(batches=100, tile_ra_rows=-1))
+    assert p.tr_rd == p.tr_tt == 0 and p.tr_a * p.tz_a > base.tr_a * base.tz_a
+    p = tmc.plan(skin, tmc.options(batches=100, tile_ra_rows=10))
+    assert p.tr_rd == p.tr_tt == 10
+    p = tmc.plan(skin, tmc.options(batches=100, tile_cross=-1))
+    assert p.cross == 0 and p.tr_a * p.tz_a > base.tr_a * base.tz_a
+    for tz in (0, 1, 17, 400):
+        for rows in (-1, 0, 3, 500):
+            for cross in (-1, 0, 1):
+                for bps in (1, 2, 3, 4):
+                    q = tmc.plan(skin, tmc.options(batches=100, tile_tz=tz, tile_ra_rows=rows, tile_cross=cross),
+                                 regs_blocks_per_sm=bps)
+                    assert q.smem_bytes <= min(232448, 233472 // bps - 1024)
+                    assert 0 <= q.tr_a <= 500 and 0 <= q.tz_a <= 400 and 0 <= q.tr_rd <= 500
+    for bad, msg in (({"tile_tz": -1}, "tile_tz"), ({"tile_ra_rows": -2}, "tile_ra_rows"),
+                     ({"tile_cross": 2}, "tile_cross")):
+        with pytest.raises(tmc.ConfigError, match=msg):
+            tmc.plan(skin, tmc.options(batches=100, **bad))
+
+
 def test_plan_smem_per_block_never_exceeds_the_device():
     rng = np.random.default_rng(0)
     for _ in range(200):

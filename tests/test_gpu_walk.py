@@ -384,6 +384,24 @@ def test_skin5_profile_bins_vs_an_independent_float64_run(skin, skin_f64):
         assert fam.passed, (k, str(fam))
 
 
+def test_autotuned_plan_gives_the_same_tallies(skin):
+    """tmc_b200_autotune searches blocks per SM, block size and the shared tile shapes on a sample of
+    the run; whatever it picks, the run's integer tallies are the same bits (only where they are
+    summed changes), and the chosen plan is never slower on the sample than the planner's default."""
+    opt = tmc.options(photons=2_000_000, batches=20, seed=4)
+    tuned, plan, t_default, t_best = tmc.autotune(skin, opt, sample_photons=2_000_000)
+    assert t_best <= t_default
+    assert plan["smem_bytes"] > 0 and plan["grid"] > 0
+    a = tmc.run(skin, opt)
+    b = tmc.run(skin, tuned)
+    assert np.array_equal(a.raw, b.raw)
+    # the tile options on their own, each away from the planner's choice
+    for kw in ({"tile_cross": -1}, {"tile_ra_rows": -1}, {"tile_tz": 399}, {"blocks_per_sm": 2},
+               {"threads_per_block": 128}):
+        o = tmc.options(photons=300_000, batches=20, seed=4, **kw)
+        assert np.array_equal(tmc.run(skin, o).raw, tmc.run(skin, photons=300_000, batches=20, seed=4).raw), kw
+
+
 # ---------------------------------------------------------------- failure paths and errors
 def test_step_cap_turns_endless_packets_into_anomalies(slab):
     """The per-photon step cap (tmc_options.step_cap) ends a packet that is still alive after that

@@ -76,6 +76,9 @@ class COptions(ctypes.Structure):
         ("blocks_per_sm", ctypes.c_int32),
         ("smem_budget", ctypes.c_int32),
         ("step_cap", ctypes.c_uint32),
+        ("tile_tz", ctypes.c_int32),
+        ("tile_ra_rows", ctypes.c_int32),
+        ("tile_cross", ctypes.c_int32),
     ]
 
 
@@ -209,6 +212,8 @@ PROTOTYPES = {
                                                   ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_int32, ctypes.c_float] + [ctypes.c_void_p] * 5 +
                                    [_P(CStatus)]),
+    "tmc_b200_autotune": (ctypes.c_int, [_P(CRunSpec), _P(COptions), ctypes.c_uint64, _P(CPlan), _pd, _pd,
+                                         _P(CStatus)]),
     "tmc_b200_plan": (ctypes.c_int, [_P(CRunSpec), _P(COptions), ctypes.c_int32, ctypes.c_int64,
                                      ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _P(CPlan),
                                      _P(CStatus)]),
@@ -287,14 +292,33 @@ class RunSpec:
 
 def options(seed: int = 1, batches: int = 10, photons: int = 0, rung: int = 0, profiles: bool = True,
             device: int = 0, fast_math: bool = True, threads_per_block: int = 0, blocks_per_sm: int = 0,
-            smem_budget: int = 0, step_cap: int = 0) -> COptions:
+            smem_budget: int = 0, step_cap: int = 0, tile_tz: int = 0, tile_ra_rows: int = 0,
+            tile_cross: int = 0) -> COptions:
     o = COptions()
     lib().tmc_b200_default_options(ctypes.byref(o))
     o.seed, o.batches, o.photons, o.rung = seed, batches, photons, rung
     o.profiles, o.device, o.fast_math = int(profiles), device, int(fast_math)
     o.threads_per_block, o.blocks_per_sm, o.smem_budget = threads_per_block, blocks_per_sm, smem_budget
     o.step_cap = step_cap
+    o.tile_tz, o.tile_ra_rows, o.tile_cross = tile_tz, tile_ra_rows, tile_cross
     return o
+
+
+def plan_dict(p: CPlan) -> dict:
+    return {k: int(getattr(p, k)) for k, _ in CPlan._fields_}
+
+
+def autotune(spec: RunSpec, opt: COptions, sample_photons: int = 20_000_000) -> tuple[COptions, dict, float, float]:
+    """Autotune the walk's launch and tally-tile plan on a sample of this run (tmc_b200_autotune):
+    returns the tuned options (a copy), the chosen plan, and the sample's kernel seconds with the
+    planner's default plan and with the chosen one."""
+    o = COptions.from_buffer_copy(opt)
+    plan, st = CPlan(), CStatus()
+    t0, t1 = ctypes.c_double(), ctypes.c_double()
+    c = spec.to_c()
+    _check(lib().tmc_b200_autotune(ctypes.byref(c), ctypes.byref(o), sample_photons, ctypes.byref(plan),
+                                   ctypes.byref(t0), ctypes.byref(t1), ctypes.byref(st)), st)
+    return o, plan_dict(plan), t0.value, t1.value
 
 
 @dataclass

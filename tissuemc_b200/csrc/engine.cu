@@ -135,7 +135,7 @@ Plan make_plan(const tmc_run_spec &spec, const tmc_options &opt, const DeviceLim
                         : std::min(lim.smem_block_optin, lim.smem_sm / static_cast<size_t>(bps) - lim.reserved);
     budget &= ~static_cast<size_t>(15);
     const size_t layer_bytes = ((static_cast<size_t>(sh.nl) * sizeof(LayerC) + 15) / 16) * 16;
-    const size_t ring_bytes = 32 * static_cast<size_t>(p.threads);  // 8 random words per lane
+    const size_t ring_bytes = 4 * kRingWords * static_cast<size_t>(p.threads);  // random words per lane
     budget = std::max(budget, layer_bytes + ring_bytes + 16);
     size_t rem = budget - layer_bytes - ring_bytes - 16;
     const size_t batch_bytes = static_cast<size_t>(sh.nb) * (4 + sh.nl) * 8;
@@ -149,15 +149,27 @@ Plan make_plan(const tmc_run_spec &spec, const tmc_options &opt, const DeviceLim
             p.tz_a = sh.nz;
             p.tr_rd = p.tr_tt = sh.nr;
         } else {
-            const size_t ra_each = std::min(full_ra, rem / 8);
-            p.tr_rd = p.tr_tt = static_cast<int>(ra_each / (na * 8));
-            rem -= 2 * static_cast<size_t>(p.tr_rd) * na * 8;
+            // rows of R_d(r,a) and T_t(r,a): an eighth of the budget each, or as the options say
+            size_t rows = std::min(full_ra, rem / 8) / (na * 8);
+            if (opt.tile_ra_rows == -1) rows = 0;
+            if (opt.tile_ra_rows > 0) rows = std::min<size_t>({nr, static_cast<size_t>(opt.tile_ra_rows), rem / 2 / (na * 8)});
+            p.tr_rd = p.tr_tt = static_cast<int>(rows);
+            rem -= 2 * rows * na * 8;
             const size_t cross = (nr + nz) * 8;
-            if (rem >= cross) {
+            const bool want_cross = opt.tile_cross != -1;
+            if (want_cross && rem >= cross) {
                 p.cross = 1;
-                const size_t core = (rem - cross) / 8;
-                size_t tz = std::min<size_t>(nz - 1, static_cast<size_t>(2.0 * std::sqrt(static_cast<double>(core))));
-                size_t tr = tz > 0 ? std::min<size_t>(nr - 1, core / tz) : 0;
+                rem -= cross;
+            }
+            if (p.cross || !want_cross) {
+                // the core tile: tz depth bins (about 2 sqrt(words), or as the options say) by as
+                // many radial rows as fit; without the cross it may reach the last row and column
+                const size_t core = rem / 8;
+                const size_t zmax = p.cross ? nz - 1 : nz, rmax = p.cross ? nr - 1 : nr;
+                size_t tz = opt.tile_tz > 0 ? static_cast<size_t>(opt.tile_tz)
+                                            : static_cast<size_t>(2.0 * std::sqrt(static_cast<double>(core)));
+                tz = std::min(tz, zmax);
+                size_t tr = tz > 0 ? std::min(rmax, core / tz) : 0;
                 if (tr == 0 || tz == 0) tr = tz = 0;
                 p.tr_a = static_cast<int>(tr);
                 p.tz_a = static_cast<int>(tz);
@@ -560,6 +572,116 @@ int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_re
         std::snprintf(res->device, sizeof res->device, "%.100s (sm_%d%d)", d.prop.name, d.prop.major,
                       d.prop.minor);
         res->wall_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return TMC_OK;
+    } catch (const ConfigFailure &e) {
+        set_status(st, TMC_BAD_CONFIG, e.what());
+        return TMC_BAD_CONFIG;
+    } catch (const Fail &e) {
+        set_status(st, e.code(), e.what());
+        return e.code();
+    } catch (const std::exception &e) {
+        set_status(st, TMC_CUDA_ERROR, e.what());
+        return TMC_CUDA_ERROR;
+    }
+}
+
+int tmc_b200_autotune(const tmc_run_spec *spec, tmc_options *opt, uint64_t sample_photons, tmc_plan *plan_out,
+                      double *default_seconds, double *best_seconds, tmc_status *st) {
+    set_status(st, TMC_OK, "");
+    if (!spec || !opt) {
+        set_status(st, TMC_BAD_ARGUMENT, "NULL argument");
+        return TMC_BAD_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    try {
+        validate_run(*spec, *opt);
+        DeviceCtx &c = device_ctx(opt->device);
+        // the sample: the run's first photons, with its seed and (at most as many) batches
+        tmc_options base = *opt;
+        const uint64_t total = shape_of(*spec, *opt).photons;
+        base.photons = std::max<uint64_t>(1, std::min<uint64_t>(total, sample_photons ? sample_photons : total));
+        base.batches = static_cast<int32_t>(std::min<uint64_t>(static_cast<uint64_t>(base.batches), base.photons));
+        ensure_tally(c, tally_offsets(shape_of(*spec, base)).total);
+        auto regs_blocks = [&](const tmc_options &o) {
+            int bps = 0;
+            const int threads = o.threads_per_block > 0 ? o.threads_per_block : 256;
+            if (o.fast_math)
+                TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, walk_kernel<1>, threads, 0));
+            else
+                TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, walk_kernel<0>, threads, 0));
+            return bps;
+        };
+        auto time_of = [&](const tmc_options &o) -> double {
+            const Plan pl = make_plan(*spec, o, limits_of(c.prop), regs_blocks(o));
+            if (plan_smem_bytes(make_params(*spec, o, pl, nullptr, nullptr)) > c.prop.sharedMemPerBlockOptin)
+                return 1e30;  // not a plan this device can run
+            double best = 1e30;
+            for (int rep = 0; rep < 3; ++rep) {  // a warm-up, then the best of two
+                launch_walk(*spec, o, c, c.d_tally, c.d_counter, c.stream, c.ev0, c.ev1);
+                TMC_CUDA(cudaStreamSynchronize(c.stream));
+                float ms = 0.f;
+                TMC_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+                if (rep) best = std::min(best, static_cast<double>(ms) / 1000.0);
+            }
+            return best;
+        };
+        const int regs_bps = regs_blocks(base);
+        const Plan p0 = make_plan(*spec, base, limits_of(c.prop), regs_bps);
+        tmc_options best = base;
+        const double t_default = time_of(best);
+        double t_best = t_default;
+        auto try_opt = [&](const tmc_options &o) {
+            const double t = time_of(o);
+            if (t < t_best * 0.995) {  // keep a change only when it is clearly faster
+                t_best = t;
+                best = o;
+            }
+        };
+        // coordinate descent: occupancy and block size first (they set the budget per block), then
+        // the tile shapes within that budget
+        for (int bps = std::max(1, regs_bps - 2); bps < regs_bps; ++bps) {
+            tmc_options o = best;
+            o.blocks_per_sm = bps;
+            try_opt(o);
+        }
+        {
+            tmc_options o = best;
+            o.threads_per_block = 128;
+            o.blocks_per_sm = 0;
+            try_opt(o);
+        }
+        {
+            tmc_options o = best;
+            o.tile_cross = -1;
+            try_opt(o);
+        }
+        const int tz0 = std::max(1, p0.tz_a);
+        for (int tz : {tz0 / 2, tz0 * 2, tz0 * 4, spec->nz}) {
+            if (tz < 1) continue;
+            tmc_options o = best;
+            o.tile_tz = tz;
+            try_opt(o);
+        }
+        const int rows0 = std::max(1, p0.tr_rd);
+        for (int rows : {-1, rows0 / 2, rows0 * 2}) {
+            if (rows == 0) continue;
+            tmc_options o = best;
+            o.tile_ra_rows = rows;
+            try_opt(o);
+        }
+        opt->threads_per_block = best.threads_per_block;
+        opt->blocks_per_sm = best.blocks_per_sm;
+        opt->tile_tz = best.tile_tz;
+        opt->tile_ra_rows = best.tile_ra_rows;
+        opt->tile_cross = best.tile_cross;
+        if (plan_out) {
+            const Plan p = make_plan(*spec, *opt, limits_of(c.prop), regs_blocks(*opt));
+            const WalkParams P = make_params(*spec, *opt, p, nullptr, nullptr);
+            *plan_out = tmc_plan{p.threads, p.blocks_per_sm, p.grid, p.tr_a, p.tz_a, p.cross, p.tr_rd, p.tr_tt,
+                                 p.batch_smem, static_cast<int32_t>(plan_smem_bytes(P))};
+        }
+        if (default_seconds) *default_seconds = t_default;
+        if (best_seconds) *best_seconds = t_best;
         return TMC_OK;
     } catch (const ConfigFailure &e) {
         set_status(st, TMC_BAD_CONFIG, e.what());

@@ -42,7 +42,8 @@ __global__ void probe_kernel(int what, Hot h, uint64_t seed, long long per_threa
     ProbeRng rng{tid, 0u, static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32), {0u, 0u, 0u, 0u}, 4};
     double s1 = 0.0, s2 = 0.0;
     float lo = 2.0f, hi = -2.0f, worst = 0.0f;
-    float ux = 0.0f, uy = 0.0f, uz = 1.0f;
+    float2 uxy = make_float2(0.0f, 0.0f);
+    float uz = 1.0f;
     for (long long i = 0; i < per_thread; ++i) {
         if (what == 0) {
             const float c = hg_cos<FAST>(h, rng.next());
@@ -52,9 +53,9 @@ __global__ void probe_kernel(int what, Hot h, uint64_t seed, long long per_threa
             hi = fmaxf(hi, c);
         } else if (what == 1) {
             const float ct = hg_cos<FAST>(h, rng.next());
-            rotate<FAST>(ux, uy, uz, ct, rng.next());
-            const float n = sqrtf(static_cast<float>(static_cast<double>(ux) * ux + static_cast<double>(uy) * uy +
-                                                     static_cast<double>(uz) * uz));
+            rotate<FAST>(uxy, uz, ct, rng.next());
+            const double ux = uxy.x, uy = uxy.y;
+            const float n = sqrtf(static_cast<float>(ux * ux + uy * uy + static_cast<double>(uz) * uz));
             worst = fmaxf(worst, fabsf(n - 1.0f));
         } else {
             const float s = step_length<FAST>(h, rng.next());

@@ -199,8 +199,8 @@ std::unique_ptr<SweepGraph> build_graph(int cap, int lmax, const tmc_sweep_optio
     g->stride = static_cast<size_t>(o.batches) * (4 + lmax) + static_cast<size_t>(o.nr) * o.nz +
                 2 * static_cast<size_t>(o.nr) * o.na;
     g->threads = o.threads_per_block > 0 ? o.threads_per_block : 256;
-    // per lane: the random-word ring (8 words) and the Philox key schedule (5 x 16 bytes)
-    g->smem = (32 + 80) * static_cast<size_t>(g->threads);
+    // per lane: the random-word ring (kRingWords words) and the Philox key schedule (5 x 16 bytes)
+    g->smem = (4 * kRingWords + 80) * static_cast<size_t>(g->threads);
     cudaDeviceProp prop;
     SW_CUDA(cudaGetDeviceProperties(&prop, o.device));
     int bps = 0;

@@ -84,7 +84,7 @@ template <int FAST> struct SweepCtx {
     }
     __device__ __forceinline__ void absorb(const Lane &L, unsigned long long v) {
         if (!P.profiles) return;
-        const float rr = radius<FAST>(L.x, L.y);
+        const float rr = radius<FAST>(L.xy);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int iz = bin_of<FAST>(L.z, P.dz, P.inv_dz, P.nz);
         const int key = t + a_off + ir * P.nz + iz;
@@ -102,7 +102,7 @@ template <int FAST> struct SweepCtx {
     }
     __device__ __forceinline__ void exit(const Lane &L, int kind, unsigned long long v) const {
         if (!P.profiles) return;
-        const float rr = radius<FAST>(L.x, L.y);
+        const float rr = radius<FAST>(L.xy);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int ia = P.na > 1 ? bin_of<FAST>(acosf(fminf(fabsf(L.uz), 1.0f)), P.da, P.inv_da, P.na) : 0;
         atomicAdd(&P.tally[t + (kind == 1 ? rd_off : tt_off) + ir * P.na + ia], v);
@@ -133,8 +133,9 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                      P.nb * (4 + P.lmax) + P.nr * P.nz + P.nr * P.na,
                      4 + P.lmax,
                      0xFFFFFFFFu,
-                     // after the rings (8 words per lane): 5 x 16 bytes of key schedule per lane
-                     reinterpret_cast<uint4 *>(reinterpret_cast<uint32_t *>(smem) + 8 * P.threads) + threadIdx.x,
+                     // after the rings (kRingWords words per lane): 5 x 16 bytes of key schedule per lane
+                     reinterpret_cast<uint4 *>(reinterpret_cast<uint32_t *>(smem) + kRingWords * P.threads) +
+                         threadIdx.x,
                      1,
                      P.layers,
                      0,

@@ -216,9 +216,18 @@ __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b)
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+// The same operations on pairs, one paired instruction each (f32x2: two independent lanes, each
+// rounded exactly as the scalar operation above), for the x/y halves of positions and directions.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
 // a^2 + b^2 + c^2 and a^2 + b^2
 __device__ __forceinline__ float norm2(float a, float b, float c) { return ffma(a, a, ffma(b, b, fmul(c, c))); }
 __device__ __forceinline__ float norm2(float a, float b) { return ffma(a, a, fmul(b, b)); }
+__device__ __forceinline__ float norm2(float2 ab, float c) { return norm2(ab.x, ab.y, c); }
+__device__ __forceinline__ float norm2(float2 ab) { return norm2(ab.x, ab.y); }
 
 __device__ __forceinline__ unsigned long long to_fixed(float w) {
     return __float2ull_rn(fmul(w, kFixedScale));

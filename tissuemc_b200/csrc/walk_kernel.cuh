@@ -21,9 +21,9 @@ struct SmemLayout {
 __host__ __device__ inline SmemLayout smem_layout(const WalkParams &P) {
     SmemLayout s;
     int off = 0;
-    // each lane's random words: a ring of 8 32-bit words
+    // each lane's random words: a ring of kRingWords 32-bit words
     s.ring = off;
-    off += 4 * static_cast<int>(P.threads);
+    off += static_cast<int>(kRingWords / 2) * static_cast<int>(P.threads);
     s.batch = off;
     off += P.batch_smem ? P.nb * (4 + P.nl) : 0;
     s.core_a = off;
@@ -94,7 +94,7 @@ template <int FAST> struct PlainCtx {
 
     __device__ __forceinline__ void absorb(const Lane &L, unsigned long long v) {
         if (!P.profiles) return;
-        const float rr = radius<FAST>(L.x, L.y);
+        const float rr = radius<FAST>(L.xy);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int iz = bin_of<FAST>(L.z, P.dz, P.inv_dz, P.nz);
         if (ir == cache_ir && iz == cache_iz) {
@@ -114,7 +114,7 @@ template <int FAST> struct PlainCtx {
 
     __device__ __forceinline__ void exit(const Lane &L, int kind, unsigned long long v) const {
         if (!P.profiles) return;
-        const float rr = radius<FAST>(L.x, L.y);
+        const float rr = radius<FAST>(L.xy);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int ia = bin_of<FAST>(acosf(fminf(fabsf(L.uz), 1.0f)), P.da, P.inv_da, P.na);
         if (kind == 1) {

@@ -19,6 +19,17 @@
 
 namespace tmc {
 
+// Random words a lane keeps in its shared-memory ring (a power of two). With 8 a lane refills one
+// Philox block as soon as fewer than the 4 words a step may draw are left, on its own. With 16 the
+// refill is warp-uniform (TMC_RING_WORDS=16): when any lane of the warp is short, every lane with
+// room for a block refills too, so the lanes of a warp refill together (fewer, fuller refills;
+// the words each photon consumes, and their order, are the same either way).
+#ifndef TMC_RING_WORDS
+#define TMC_RING_WORDS 8
+#endif
+constexpr uint32_t kRingWords = TMC_RING_WORDS;
+static_assert(kRingWords == 8 || kRingWords == 16, "ring of 8 or 16 words");
+
 constexpr float kCosZero = 1.0f - 1e-6f;  // physics.hpp:35 (float widening of MCML COSZERO)
 constexpr float kCos90D = 1e-6f;          // physics.hpp:36
 constexpr float kWeightMin = 1e-4f;       // physics.hpp:33 (MCML WEIGHT)
@@ -108,10 +119,11 @@ template <int FAST> __device__ __forceinline__ float hg_cos(const Hot &h, float 
     return fminf(fmaxf(ct, -1.0f), 1.0f);
 }
 
-// Turn the direction by the polar cosine ct and the azimuth 2 pi u, then renormalise it
-// (physics.hpp:116-144).
+// Turn the direction (u.x, u.y, uz) by the polar cosine ct and the azimuth 2 pi u, then renormalise
+// it (physics.hpp:116-144). The x and y halves go through paired instructions, each half rounded as
+// the scalar form would round it.
 template <int FAST>
-__device__ __forceinline__ void rotate(float &ux, float &uy, float &uz, float ct, float u) {
+__device__ __forceinline__ void rotate(float2 &uxy, float &uz, float ct, float u) {
     float st = ffma(-ct, ct, 1.0f);
     st = st > 0.0f ? m_sqrt<FAST>(st) : 0.0f;
     float sp, cp;
@@ -124,38 +136,38 @@ __device__ __forceinline__ void rotate(float &ux, float &uy, float &uz, float ct
         sincosf(fmul(kTwoPi, u), &sp, &cp);
     }
     if (fabsf(uz) > kCosZero) {
-        ux = fmul(st, cp);
-        uy = fmul(st, sp);
+        uxy = fmul2(f2(st), f2(cp, sp));
         uz = uz >= 0.0f ? ct : -ct;
     } else {
-        const float ox = ux, oy = uy, oz = uz;
+        const float2 o = uxy;
+        const float oz = uz;
         const float q = ffma(-oz, oz, 1.0f);  // 1 - uz^2
-        const float ix = ffma(fmul(ox, oz), cp, -fmul(oy, sp));
-        const float iy = ffma(fmul(oy, oz), cp, fmul(ox, sp));
+        // (ix, iy) = (ox oz cp - oy sp, oy oz cp + ox sp)
+        const float2 ixy = ffma2(fmul2(o, f2(oz)), f2(cp), fmul2(f2(-o.y, o.x), f2(sp)));
+        const float2 oct = fmul2(o, f2(ct));
         if constexpr (Math<FAST>::sqrt) {
             const float it = rsqrtf(q);
-            ux = ffma(fmul(st, ix), it, fmul(ox, ct));
-            uy = ffma(fmul(st, iy), it, fmul(oy, ct));
+            uxy = ffma2(fmul2(f2(st), ixy), f2(it), oct);
             uz = ffma(fmul(fmul(-st, cp), q), it, fmul(oz, ct));
         } else {
             const float tmp = sqrtf(q);
-            ux = fadd(fmul(st, ix) / tmp, fmul(ox, ct));
-            uy = fadd(fmul(st, iy) / tmp, fmul(oy, ct));
+            uxy = f2(fadd(fmul(st, ixy.x) / tmp, oct.x), fadd(fmul(st, ixy.y) / tmp, oct.y));
             uz = ffma(fmul(-st, cp), tmp, fmul(oz, ct));
         }
     }
-    const float inv = m_rsqrt<FAST>(norm2(ux, uy, uz));
-    ux = fmul(ux, inv);
-    uy = fmul(uy, inv);
+    const float inv = m_rsqrt<FAST>(norm2(uxy, uz));
+    uxy = fmul2(uxy, f2(inv));
     uz = fmul(uz, inv);
 }
 
 // Radial distance of the packet from the source axis (the r of A(r,z), R_d(r,a), T_t(r,a)).
-template <int FAST> __device__ __forceinline__ float radius(float x, float y) { return m_sqrt<FAST>(norm2(x, y)); }
+template <int FAST> __device__ __forceinline__ float radius(float2 xy) { return m_sqrt<FAST>(norm2(xy)); }
 
 // All state of one lane's current photon (registers).
 struct Lane {
-    float x, y, z, ux, uy, uz, w, sleft;
+    float2 xy;   // position across the layers (x, y) [cm]
+    float2 uxy;  // direction cosines (ux, uy)
+    float z, uz, w, sleft;
     int layer, batch;
     uint32_t id, blk, rp, wp;  // photon id, Philox block, ring read/write positions
     uint32_t events, anomalies, steps;
@@ -169,8 +181,9 @@ __device__ __forceinline__ void launch(Lane &L, Ctx &C, uint32_t id, int batch, 
     L.id = id;
     L.blk = 0u;
     L.rp = L.wp = 0u;
-    L.x = L.y = L.z = 0.f;
-    L.ux = L.uy = 0.f;
+    L.xy = f2(0.f);
+    L.z = 0.f;
+    L.uxy = f2(0.f);
     L.uz = 1.f;
     L.w = launch_w;
     L.sleft = 0.f;
@@ -184,7 +197,12 @@ __device__ __forceinline__ void launch(Lane &L, Ctx &C, uint32_t id, int batch, 
 // One hop-drop-spin (or boundary) step plus roulette; returns true when the packet has ended
 // (its per-photon totals are then published).
 template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L, Ctx &C) {
-    if (L.wp - L.rp < 4u) C.refill(L);  // a step draws at most 4 words
+    if constexpr (kRingWords == 8) {
+        if (L.wp - L.rp < 4u) C.refill(L);  // a step draws at most 4 words
+    } else {
+        // warp-uniform: the lanes stepping together refill together when any of them is short
+        if (__any_sync(__activemask(), L.wp - L.rp < 4u) && L.wp - L.rp <= kRingWords - 4u) C.refill(L);
+    }
     ++L.steps;
     float s;
     if (L.sleft == 0.0f) {
@@ -203,8 +221,7 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
             hit = true;
         }
     }
-    L.x = ffma(s, L.ux, L.x);
-    L.y = ffma(s, L.uy, L.y);
+    L.xy = ffma2(f2(s), L.uxy, L.xy);
     L.z = ffma(s, L.uz, L.z);
 
     bool died = false;
@@ -221,8 +238,7 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
                             ? 1.0f
                             : fresnel<FAST>(Lc.n, nt, ca1, up ? Lc.rn_up : Lc.rn_dn, rat, uz1);
         if (unit_open(C.draw(L)) > r) {
-            L.ux = fmul(L.ux, rat);
-            L.uy = fmul(L.uy, rat);
+            L.uxy = fmul2(L.uxy, f2(rat));
             L.uz = up ? -uz1 : uz1;
             if (up ? L.layer == 0 : L.layer == C.num_layers(L) - 1) {
                 exit_kind = up ? 1 : 2;
@@ -246,7 +262,7 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
         L.w = fsub(L.w, dwa);
         ++L.events;
         {
-            const float n2 = norm2(L.ux, L.uy, L.uz);
+            const float n2 = norm2(L.uxy, L.uz);
             if (!(dwa == dwa) || !(fabsf(fsub(n2, 1.0f)) <= 1e-5f)) ++L.anomalies;
         }
         const unsigned long long v = to_fixed(dwa);
@@ -254,12 +270,12 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
         C.absorb(L, v);
         // ---- spin (physics.hpp:101-144)
         const float ct = hg_cos<FAST>(L.h, unit_open(C.draw(L)));
-        rotate<FAST>(L.ux, L.uy, L.uz, ct, unit_open(C.draw(L)));
+        rotate<FAST>(L.uxy, L.uz, ct, unit_open(C.draw(L)));
     }
 
     if (exit_kind) {
         // ---- score the exit (check, totals, R_d(r,a) or T_t(r,a))
-        const float n2 = norm2(L.ux, L.uy, L.uz);
+        const float n2 = norm2(L.uxy, L.uz);
         if (!(L.w == L.w) || !(fabsf(fsub(n2, 1.0f)) <= 1e-5f)) ++L.anomalies;
         const unsigned long long v = to_fixed(L.w);
         C.batch_add(L, exit_kind - 1, v);
@@ -287,20 +303,20 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
     return died;
 }
 
-// The random-word ring: 8 words per lane in shared memory, slot k of a block's lanes contiguous
-// (ring[k * stride]), so lanes reading different slots never conflict on a bank.
+// The random-word ring: kRingWords words per lane in shared memory, slot k of a block's lanes
+// contiguous (ring[k * stride]), so lanes reading different slots never conflict on a bank.
 struct Ring {
     uint32_t *base;  // this lane's slot 0
     int stride;      // lanes per block
 
     __device__ __forceinline__ uint32_t draw(Lane &L) const {
-        const uint32_t o = base[(L.rp & 7u) * stride];
+        const uint32_t o = base[(L.rp & (kRingWords - 1u)) * stride];
         ++L.rp;
         return o;
     }
     __device__ __forceinline__ void store(Lane &L, uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3) const {
         ++L.blk;
-        uint32_t *const slot = base + (L.wp & 4u) * stride;  // wp is a multiple of 4
+        uint32_t *const slot = base + (L.wp & (kRingWords - 4u)) * stride;  // wp is a multiple of 4
         slot[0] = b0;
         slot[stride] = b1;
         slot[2 * stride] = b2;
