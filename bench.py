@@ -82,6 +82,8 @@ def _args():
     ap.add_argument("--photon-scale", type=float, default=1.0, help="sweep: scale every configuration's photons "
                     "(diagnostic)")
     ap.add_argument("--no-loop", action="store_true", help="sweep: skip the single-run loop baseline (diagnostic)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="walk: use the planner's default launch and tile plan instead of autotuning it")
     ap.add_argument("--no-extras", action="store_true",
                     help="default line only: skip the sweep, serve and reference-GPU sub-measurements")
     ap.add_argument("--no-profiles", action="store_true",
@@ -295,8 +297,20 @@ def measure_sweep(configs: int, steps: int, warmup: int, device: int, seed: int 
         for c in cfgs:
             c.photons = max(1, int(c.photons * photon_scale))
     opt = tmc.sweep_options(device=device)
+    tuned = None
     if autotune:
-        opt, _ = tmc.sweep_autotune(cfgs, opt)
+        # the launch shape and per-warp tile, timed on the same configurations at a tenth of their
+        # photons (tmc_b200_sweep_autotune); the results do not depend on them
+        sample = (tmc.CSweepConfig * len(cfgs))()
+        for i, c in enumerate(cfgs):
+            sample[i] = c
+            sample[i].photons = max(int(opt.batches), int(c.photons) // 10)
+        t_default = min(tmc.sweep_run(sample, opt).seconds for _ in range(2))
+        opt, t_best = tmc.sweep_autotune(sample, opt)
+        tuned = {"sample": "the same configurations at a tenth of their photons",
+                 "sample_seconds_default": t_default, "sample_seconds_chosen": t_best,
+                 "options": {k: int(getattr(opt, k)) for k in ("threads_per_block", "item_photons", "tile_r",
+                                                                "tile_z")}}
     for _ in range(warmup):
         tmc.sweep_run(cfgs, opt)
     with Clocks(device) as clk:
@@ -320,7 +334,8 @@ def measure_sweep(configs: int, steps: int, warmup: int, device: int, seed: int 
         "ms_per_step": 1e3 * ks, "steps": steps, "warmup": warmup,
         "config": {"workload": f"sweep: {SWEEP_DESC}", "configs": n, "photon_scale": photon_scale,
                    "threads_per_block": opt.threads_per_block, "item_photons": opt.item_photons,
-                   "autotuned": bool(autotune)},
+                   "tile_r": opt.tile_r, "tile_z": opt.tile_z, "autotuned": bool(autotune)},
+        "autotune": tuned,
         "e2e": {"value": n / ws, "unit": "solves/s",
                 "h2d_bytes_per_step": n * 48 + n * 4 + sum(c.num_layers for c in cfgs) * 96,
                 "d2h_bytes_per_step": n * (opt.nr + 3) * 8},
@@ -531,6 +546,15 @@ def main() -> None:
     first, count = tmc.shard_range(spec.photons, rank, world)
     opt = tmc.options(batches=a.batches, seed=1, device=local, rung=6 if a.no_profiles else 0,
                       profiles=not a.no_profiles)
+    tuning = None
+    if not a.no_autotune:
+        # the launch and tally-tile plan, picked by timing candidates on a 2e7-photon sample of
+        # this run (tmc_b200_autotune); the results do not depend on it
+        opt, plan, t_default, t_best = tmc.autotune(spec, opt, sample_photons=min(spec.photons, 20_000_000))
+        tuning = {"plan": plan, "sample_photons": min(spec.photons, 20_000_000),
+                  "sample_seconds_default_plan": t_default, "sample_seconds_chosen_plan": t_best,
+                  "options": {k: int(getattr(opt, k)) for k in ("threads_per_block", "blocks_per_sm", "tile_tz",
+                                                                 "tile_ra_rows", "tile_cross")}}
     sizes = tmc.query_sizes(spec, opt)
     words = int(sizes.tally_words)
     # the tallies, then the launch's photon-claim counter (device_words = tally_words + 1)
@@ -636,6 +660,7 @@ def main() -> None:
             },
             "clocks": clk.summary(),
             "kernel_ms_per_step": ms,
+            "autotune": tuning,
             "device": res.device,
         }  # fmt: skip
         if not a.no_cpu_baseline and world == 1:
@@ -652,7 +677,7 @@ def main() -> None:
             if "value" in ref_gpu:
                 ref_gpu["b200_kernel_speedup"] = value / ref_gpu["value"]
             line["reference_gpu"] = ref_gpu
-            for key, fn in (("sweep", lambda: measure_sweep(4096, 2, 1, local)),
+            for key, fn in (("sweep", lambda: measure_sweep(4096, 2, 1, local, autotune=not a.no_autotune)),
                             ("serve", lambda: measure_serve(1 << 20, 5, 3, local))):
                 try:
                     line[key] = fn()

@@ -263,6 +263,9 @@ typedef struct {
     int32_t device;
     int32_t threads_per_block; /* 0 = 256 */
     int32_t item_photons;      /* photons per work-queue item; 0 = 256 */
+    int32_t tile_r, tile_z;    /* per-warp shared-memory tile of A(r,z): the first tile_r x tile_z
+                                  bins of the configuration of the warp's current item (0 x 0 =
+                                  none, the default; at most 32 KB of tiles per block) */
 } tmc_sweep_options;
 
 typedef struct {
@@ -307,7 +310,8 @@ TMC_B200_API int tmc_b200_sweep_run_loop(const tmc_sweep_config *cfgs, int32_t n
                                          uint64_t *raw, double *seconds, tmc_status *status);
 
 /* Autotune the sweep's launch shape on these configurations: block size {128, 256} x photons per
- * work item {64, 256, 1024}, each timed on a second run; writes the fastest into *opt. */
+ * work item {64, 256, 1024}, then the per-warp shared tile of A(r,z) {none, 8 x 8, 16 x 16,
+ * 16 x 32} with the best of those, each timed on a second run; writes the fastest into *opt. */
 TMC_B200_API int tmc_b200_sweep_autotune(const tmc_sweep_config *cfgs, int32_t n, tmc_sweep_options *opt,
                                          double *best_seconds, tmc_status *status);
 

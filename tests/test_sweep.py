@@ -60,6 +60,11 @@ def test_sizes_and_validation_name_the_configuration():
         tmc.sweep_sizes(cfgs, opt)
     with pytest.raises(tmc.ConfigError, match="item_photons"):
         tmc.sweep_sizes(tmc.sweep_sample(3, 2), tmc.sweep_options(item_photons=-1))
+    for bad, msg in (({"tile_r": 8}, "both be 0"), ({"tile_r": -1, "tile_z": 4}, "both be 0"),
+                     ({"tile_r": 65, "tile_z": 4}, "cannot exceed the grid"),
+                     ({"tile_r": 32, "tile_z": 32}, "more than 32 KB")):
+        with pytest.raises(tmc.ConfigError, match=msg):
+            tmc.sweep_sizes(tmc.sweep_sample(3, 2), tmc.sweep_options(**bad))
 
 
 def _single_run_raw(c, opt):
@@ -157,10 +162,25 @@ def test_summaries_follow_from_the_tallies():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("tile", [(8, 8), (16, 16), (16, 32), (64, 4)])
+def test_per_warp_tile_gives_the_same_tallies(tile):
+    """Deposits of the configuration a warp is working on go to the warp's shared tile and are
+    handed to the global tallies when the warp moves to another configuration: the integer sums
+    are the same bits as without the tile (and as each configuration's single run)."""
+    cfgs = _scaled(tmc.sweep_sample(31, 200), 5000)
+    ref = tmc.sweep_run(cfgs, tmc.sweep_options(), raw=True)
+    for item in (64, 256):
+        got = tmc.sweep_run(cfgs, tmc.sweep_options(tile_r=tile[0], tile_z=tile[1], item_photons=item), raw=True)
+        assert np.array_equal(ref.raw, got.raw), (tile, item)
+        assert np.array_equal(ref.summary, got.summary)
+
+
+@pytest.mark.gpu
 def test_autotuner_picks_a_valid_shape():
     cfgs = _scaled(tmc.sweep_sample(8, 128), 2000)
     opt, best = tmc.sweep_autotune(cfgs, tmc.sweep_options())
     assert opt.threads_per_block in (128, 256) and opt.item_photons in (64, 256, 1024)
+    assert (opt.tile_r, opt.tile_z) in ((0, 0), (8, 8), (16, 16), (16, 32))
     assert best > 0
     ref = tmc.sweep_run(cfgs, tmc.sweep_options(), raw=True)
     tuned = tmc.sweep_run(cfgs, opt, raw=True)

@@ -133,7 +133,7 @@ class CAdamTensor(ctypes.Structure):
 class CSweepOptions(ctypes.Structure):
     _fields_ = [("dz", ctypes.c_double), ("dr", ctypes.c_double)] + [
         (k, ctypes.c_int32) for k in ("nz", "nr", "na", "batches", "fast_math", "profiles", "device",
-                                      "threads_per_block", "item_photons")]
+                                      "threads_per_block", "item_photons", "tile_r", "tile_z")]
 
 
 class CSweepSizes(ctypes.Structure):
@@ -677,7 +677,8 @@ def sweep_run_loop(cfgs, opt: CSweepOptions | None = None, raw: bool = False) ->
 
 
 def sweep_autotune(cfgs, opt: CSweepOptions | None = None) -> tuple[CSweepOptions, float]:
-    """Pick the sweep's block size and work-item size by timing candidates on these configurations."""
+    """Pick the sweep's block size, work-item size and per-warp tile of A(r,z) by timing candidates
+    on these configurations."""
     opt = opt or sweep_options()
     best = ctypes.c_double(0.0)
     st = CStatus()

@@ -89,6 +89,12 @@ SweepShape validate_sweep(const tmc_sweep_config *cfgs, int n, const tmc_sweep_o
     if (o.threads_per_block < 0 || o.threads_per_block > 256 || o.threads_per_block % 32 != 0)
         throw ConfigFailure("threads_per_block must be a multiple of 32 in [32, 256] (0 = 256)");
     if (o.item_photons < 0) throw ConfigFailure("item_photons must be >= 0 (0 = 256)");
+    if (o.tile_r < 0 || o.tile_z < 0 || (o.tile_r == 0) != (o.tile_z == 0))
+        throw ConfigFailure("tile_r and tile_z must both be 0 (no tile) or both positive");
+    if (o.tile_r > o.nr || o.tile_z > o.nz) throw ConfigFailure("the sweep's tile cannot exceed the grid");
+    const int threads = o.threads_per_block > 0 ? o.threads_per_block : 256;
+    if (static_cast<size_t>(threads / 32) * o.tile_r * o.tile_z * 8 > 32768)
+        throw ConfigFailure("the sweep's tiles take more than 32 KB of shared memory per block");
     SweepShape sh{n, 1, 0};
     for (int i = 0; i < n; ++i) {
         try {
@@ -178,7 +184,8 @@ size_t align_up(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 bool same_shape(const tmc_sweep_options &a, const tmc_sweep_options &b) {
     return a.dz == b.dz && a.dr == b.dr && a.nz == b.nz && a.nr == b.nr && a.na == b.na &&
            a.batches == b.batches && a.fast_math == b.fast_math && a.profiles == b.profiles &&
-           a.device == b.device && a.threads_per_block == b.threads_per_block;
+           a.device == b.device && a.threads_per_block == b.threads_per_block && a.tile_r == b.tile_r &&
+           a.tile_z == b.tile_z;
 }
 
 // Build (allocate, capture, instantiate) a sweep graph for up to cap configurations with up to
@@ -199,10 +206,16 @@ std::unique_ptr<SweepGraph> build_graph(int cap, int lmax, const tmc_sweep_optio
     g->stride = static_cast<size_t>(o.batches) * (4 + lmax) + static_cast<size_t>(o.nr) * o.nz +
                 2 * static_cast<size_t>(o.nr) * o.na;
     g->threads = o.threads_per_block > 0 ? o.threads_per_block : 256;
-    // per lane: the random-word ring (kRingWords words) and the Philox key schedule (5 x 16 bytes)
-    g->smem = (4 * kRingWords + 80) * static_cast<size_t>(g->threads);
+    // per lane: the random-word ring (kRingWords words) and the Philox key schedule (5 x 16 bytes);
+    // per warp: the optional tile of A(r,z)
+    g->smem = (4 * kRingWords + 80) * static_cast<size_t>(g->threads) +
+              static_cast<size_t>(g->threads / 32) * o.tile_r * o.tile_z * 8;
     cudaDeviceProp prop;
     SW_CUDA(cudaGetDeviceProperties(&prop, o.device));
+    SW_CUDA(cudaFuncSetAttribute(sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(g->smem)));
+    SW_CUDA(cudaFuncSetAttribute(sweep_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(g->smem)));
     int bps = 0;
     if (o.fast_math)
         SW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, sweep_kernel<1>, g->threads, g->smem));
@@ -247,6 +260,8 @@ std::unique_ptr<SweepGraph> build_graph(int cap, int lmax, const tmc_sweep_optio
     P.profiles = o.profiles ? 1 : 0;
     P.step_cap = 2000000000u;
     P.threads = static_cast<uint32_t>(g->threads);
+    P.tile_r = o.profiles ? o.tile_r : 0;
+    P.tile_z = o.profiles ? o.tile_z : 0;
 
     cudaGraph_t graph = nullptr;
     SW_CUDA(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
@@ -586,6 +601,24 @@ int tmc_b200_sweep_autotune(const tmc_sweep_config *cfgs, int32_t n, tmc_sweep_o
                 best_t = secs;
                 best = o;
             }
+        }
+    }
+    // then the per-warp tile of A(r,z), with the best launch shape
+    const int tiles[][2] = {{8, 8}, {16, 16}, {16, 32}};
+    for (const auto &tl : tiles) {
+        tmc_sweep_options o = best;
+        o.tile_r = std::min(tl[0], o.nr);
+        o.tile_z = std::min(tl[1], o.nz);
+        const int th = o.threads_per_block > 0 ? o.threads_per_block : 256;
+        if (static_cast<size_t>(th / 32) * o.tile_r * o.tile_z * 8 > 32768) continue;
+        double secs = 0;
+        for (int rep = 0; rep < 2; ++rep) {
+            const int rc = tmc_b200_sweep_run(cfgs, n, &o, nullptr, nullptr, &secs, st);
+            if (rc != TMC_OK) return rc;
+        }
+        if (secs < best_t * 0.995) {
+            best_t = secs;
+            best = o;
         }
     }
     *opt = best;

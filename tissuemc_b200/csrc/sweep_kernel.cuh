@@ -18,6 +18,13 @@
 // to drain. Tallies of configuration c live at tally + c * stride in the single-run layout (batch
 // totals, A(r,z), R_d(r,a), T_t(r,a)), accumulated with 64-bit integer atomics in global memory
 // (L2); a per-lane run cache merges consecutive deposits into one bin.
+//
+// Optionally (tile_r x tile_z > 0) each warp privatises the first tile_r x tile_z bins of A(r,z) of
+// one configuration, the one of the item it took last, in shared memory: deposits of its lanes'
+// photons of that configuration into those bins are shared-memory atomics. When the warp takes an
+// item of another configuration, its lanes first hand any pending run-cache value for the tile
+// over, then the warp adds the tile's non-zero words into the configuration's global tallies and
+// clears it (integer sums: the totals are the same whichever way they are summed).
 #pragma once
 
 #include "walk_step.cuh"
@@ -58,7 +65,10 @@ struct SweepParams {
     int profiles;
     uint32_t step_cap;
     uint32_t threads;
+    int tile_r, tile_z;             // per-warp shared tile of A(r,z) (0: none)
 };
+
+constexpr int kNoCacheKey = 0x7FFFFFFF;  // the run cache is empty (tally word indices stay below)
 
 template <int FAST> struct SweepCtx {
     const SweepParams &P;
@@ -71,9 +81,14 @@ template <int FAST> struct SweepCtx {
     int nl;
     const LayerC *layers;
     int t;  // word offset of the configuration's tallies in P.tally (they hold < 2^31 words)
-    // run cache: word index into P.tally of the last A(r,z) bin, and its pending value
+    // run cache: word index into P.tally of the last A(r,z) bin (or -1 - its index in the warp's
+    // tile), and its pending value
     int cache_key;
     unsigned long long cache_val;
+    // the warp's tile (warp-uniform): its words, and the configuration it holds (none: 0xFFFFFFFF)
+    unsigned long long *tile;
+    uint32_t tile_cfg;
+    int tile_t;  // tally offset of tile_cfg
 
     __device__ __forceinline__ void refill(Lane &L) const { ring.refill(L, sched, static_cast<int>(P.threads)); }
     __device__ __forceinline__ uint32_t draw(Lane &L) const { return ring.draw(L); }
@@ -82,23 +97,46 @@ template <int FAST> struct SweepCtx {
     __device__ __forceinline__ void batch_add(const Lane &L, int slot, unsigned long long v) const {
         atomicAdd(&P.tally[t + L.batch * bstride + slot], v);
     }
+    __device__ __forceinline__ void deposit(int key, unsigned long long v) const {
+        if (key < 0) atomicAdd(&tile[-1 - key], v);
+        else atomicAdd(&P.tally[key], v);
+    }
     __device__ __forceinline__ void absorb(const Lane &L, unsigned long long v) {
         if (!P.profiles) return;
         const float rr = radius<FAST>(L.xy);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int iz = bin_of<FAST>(L.z, P.dz, P.inv_dz, P.nz);
-        const int key = t + a_off + ir * P.nz + iz;
+        const int key = (cfg == tile_cfg && ir < P.tile_r && iz < P.tile_z) ? -1 - (ir * P.tile_z + iz)
+                                                                            : t + a_off + ir * P.nz + iz;
         if (key == cache_key) {
             cache_val += v;
         } else {
-            if (cache_key >= 0) atomicAdd(&P.tally[cache_key], cache_val);
+            if (cache_key != kNoCacheKey) deposit(cache_key, cache_val);
             cache_key = key;
             cache_val = v;
         }
     }
     __device__ __forceinline__ void flush_cache() {
-        if (cache_key >= 0) atomicAdd(&P.tally[cache_key], cache_val);
-        cache_key = -1;
+        if (cache_key != kNoCacheKey) deposit(cache_key, cache_val);
+        cache_key = kNoCacheKey;
+    }
+    // Whole warp: hand the tile's sums to the global tallies of its configuration and clear it.
+    __device__ __forceinline__ void flush_tile(unsigned lane) {
+        if (cache_key < 0) {  // a pending run-cache value aimed at the tile
+            atomicAdd(&tile[-1 - cache_key], cache_val);
+            cache_key = kNoCacheKey;
+        }
+        __syncwarp();
+        if (tile_cfg != 0xFFFFFFFFu) {
+            for (int i = static_cast<int>(lane); i < P.tile_r * P.tile_z; i += 32) {
+                const unsigned long long w = tile[i];
+                if (w) {
+                    atomicAdd(&P.tally[tile_t + a_off + (i / P.tile_z) * P.nz + i % P.tile_z], w);
+                    tile[i] = 0ull;
+                }
+            }
+        }
+        __syncwarp();
     }
     __device__ __forceinline__ void exit(const Lane &L, int kind, unsigned long long v) const {
         if (!P.profiles) return;
@@ -139,9 +177,17 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                      1,
                      P.layers,
                      0,
-                     -1,
-                     0ull};
+                     kNoCacheKey,
+                     0ull,
+                     // after the key schedules: one tile per warp
+                     reinterpret_cast<unsigned long long *>(reinterpret_cast<uint32_t *>(smem) +
+                                                            (kRingWords + 20) * P.threads) +
+                         static_cast<size_t>(threadIdx.x >> 5) * P.tile_r * P.tile_z,
+                     0xFFFFFFFFu,
+                     0};
     const unsigned lane = threadIdx.x & 31u;
+    for (int i = static_cast<int>(lane); i < P.tile_r * P.tile_z; i += 32) C.tile[i] = 0ull;
+    __syncwarp();
     const unsigned lt_mask = (1u << lane) - 1u;
     const SweepHeader &H = *P.hdr;  // read where an item is taken (rare), not held in registers
 
@@ -150,10 +196,17 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
     bool items_done = false;
     unsigned ex_mask = 0u;  // warp-uniform: lanes with no photon left to take
     bool alive = false;
+    bool held = false;  // L holds a photon whose totals are not yet published (kPublishAtRelaunch)
     Lane L;
 
     for (;;) {
         unsigned need = ~__ballot_sync(0xffffffffu, alive) & ~ex_mask;
+        if constexpr (kPublishAtRelaunch) {
+            if (((need >> lane) & 1u) && held) {  // the lane's last photon ended: publish it
+                finish_photon(L, C);
+                held = false;
+            }
+        }
         while (need) {  // warp-uniform: hand out photons, taking new items as they run out
             const uint32_t avail = it_end - it_next;
             if (avail == 0u) {
@@ -165,6 +218,11 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                     if (idx < H.order.total) {
                         sweep_item(idx, H.order, H.item_photons, H.n_cfg, P.prefix,
                                    [&](uint32_t c) { return P.cfgs[c].photons; }, it_cfg, it_next, it_end);
+                        if (P.tile_r > 0 && it_cfg != C.tile_cfg) {  // the tile follows the warp's item
+                            C.flush_tile(lane);
+                            C.tile_cfg = it_cfg;
+                            C.tile_t = static_cast<int>(it_cfg) * P.stride;
+                        }
                         continue;
                     }
                     items_done = true;
@@ -189,15 +247,26 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                 const int batch = batch_of(id, cf.plan_base, cf.plan_extra, cf.plan_bnd);
                 launch(L, C, id, batch, cf.launch_w);
                 alive = true;
+                held = true;
             }
             need &= ~__ballot_sync(0xffffffffu, mine);
             it_next += take;
         }
         if (ex_mask == 0xffffffffu) break;  // exhausted lanes hold no photon: the warp is done
-        if (!alive) continue;
-        if (walk_step<FAST>(L, C)) alive = false;
+        if constexpr (kDeferBoundary > 0) {
+            // lanes waiting on a boundary cross together once enough of them (or all) wait
+            const unsigned live = __ballot_sync(0xffffffffu, alive);
+            const unsigned pend = __ballot_sync(0xffffffffu, alive && L.pending);
+            const bool boundaries = pend != 0u && (__popc(pend) >= kDeferBoundary || pend == live);
+            if (!alive) continue;
+            if (walk_step_deferred<FAST>(L, C, boundaries)) alive = false;
+        } else {
+            if (!alive) continue;
+            if (walk_step<FAST>(L, C)) alive = false;
+        }
     }
     C.flush_cache();
+    if (P.tile_r > 0) C.flush_tile(lane);
 }
 
 // Per-configuration summaries from the integer tallies, in double: R_d(r) per photon (nr values,

@@ -162,7 +162,12 @@ __device__ __forceinline__ void philox4x32_10_sched(uint32_t c0, uint32_t c1, ui
 // (2m + 1) 2^-24 exactly (an odd integer below 2^24 times a power of two), bit for bit the
 // reference's value.
 __device__ __forceinline__ float unit_open(uint32_t x) {
+#if TMC_UNIT_ADD
+    // the same bits: (x >> 9) has no bit in common with the exponent pattern, so + equals |
+    return __fsub_rn(__uint_as_float((x >> 9) + 0x3F800000u), 0x1.fffffep-1f);
+#else
     return __fsub_rn(__uint_as_float((x >> 9) | 0x3F800000u), 0x1.fffffep-1f);
+#endif
 }
 
 // ------------------------------------------------------------------------------------ math

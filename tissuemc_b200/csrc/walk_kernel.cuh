@@ -97,6 +97,10 @@ template <int FAST> struct PlainCtx {
         const float rr = radius<FAST>(L.xy);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int iz = bin_of<FAST>(L.z, P.dz, P.inv_dz, P.nz);
+#if TMC_NO_RUN_CACHE
+        deposit(ir, iz, v);
+        return;
+#endif
         if (ir == cache_ir && iz == cache_iz) {
             cache_val += v;
         } else {
@@ -173,12 +177,19 @@ __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P
     WarpPool pool;                           // warp-uniform photon-id pool
     unsigned ex_mask = 0u;                   // warp-uniform: lanes with no photon left to take
     bool alive = false;
+    bool held = false;  // L holds a photon whose totals are not yet published (kPublishAtRelaunch)
     Lane L;
 
     for (;;) {
         // ---- relaunch: lanes without a photon take the next ids from the warp's pool
         const unsigned need = ~__ballot_sync(0xffffffffu, alive) & ~ex_mask;
         if (need) {
+            if constexpr (kPublishAtRelaunch) {
+                if (((need >> lane) & 1u) && held) {  // the lane's last photon ended: publish it
+                    finish_photon(L, C);
+                    held = false;
+                }
+            }
             const uint32_t n = static_cast<uint32_t>(__popc(need));
             const uint32_t rank = static_cast<uint32_t>(__popc(need & lt_mask));
             uint32_t base = 0u;
@@ -194,11 +205,21 @@ __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P
                 const uint32_t id = P.id_base + my;  // the run's photon id: its stream and its batch
                 launch(L, C, id, batch_of(id, P.plan_base, P.plan_extra, P.plan_bnd), P.launch_w);
                 alive = true;
+                held = true;
             }
         }
         if (ex_mask == 0xffffffffu) break;  // exhausted lanes hold no photon: the warp is done
-        if (!alive) continue;
-        if (walk_step<FAST>(L, C)) alive = false;
+        if constexpr (kDeferBoundary > 0) {
+            // lanes waiting on a boundary cross together once enough of them (or all) wait
+            const unsigned live = __ballot_sync(0xffffffffu, alive);
+            const unsigned pend = __ballot_sync(0xffffffffu, alive && L.pending);
+            const bool boundaries = pend != 0u && (__popc(pend) >= kDeferBoundary || pend == live);
+            if (!alive) continue;
+            if (walk_step_deferred<FAST>(L, C, boundaries)) alive = false;
+        } else {
+            if (!alive) continue;
+            if (walk_step<FAST>(L, C)) alive = false;
+        }
     }
     C.flush_cache();
 

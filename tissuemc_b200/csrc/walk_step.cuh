@@ -19,13 +19,14 @@
 
 namespace tmc {
 
-// Random words a lane keeps in its shared-memory ring (a power of two). With 8 a lane refills one
-// Philox block as soon as fewer than the 4 words a step may draw are left, on its own. With 16 the
-// refill is warp-uniform (TMC_RING_WORDS=16): when any lane of the warp is short, every lane with
-// room for a block refills too, so the lanes of a warp refill together (fewer, fuller refills;
-// the words each photon consumes, and their order, are the same either way).
+// Random words a lane keeps in its shared-memory ring (a power of two). With 16 (the default) the
+// refill is warp-uniform: when any lane of the warp has fewer than the 4 words a step may draw,
+// every lane with room for a block refills too, so the lanes of a warp refill together (0.75
+// refills per step with all 32 lanes busy, against 1 per step with 24 of them when each lane
+// refills on its own; measured 4.3 % faster on skin5). With 8 a lane refills alone. The words each
+// photon consumes, and their order, are the same either way.
 #ifndef TMC_RING_WORDS
-#define TMC_RING_WORDS 8
+#define TMC_RING_WORDS 16
 #endif
 constexpr uint32_t kRingWords = TMC_RING_WORDS;
 static_assert(kRingWords == 8 || kRingWords == 16, "ring of 8 or 16 words");
@@ -171,6 +172,7 @@ struct Lane {
     int layer, batch;
     uint32_t id, blk, rp, wp;  // photon id, Philox block, ring read/write positions
     uint32_t events, anomalies, steps;
+    bool pending;                // stopped on a boundary, waiting for its warp (kDeferBoundary)
     unsigned long long run_abs;  // fixed-point weight absorbed in the current layer
     Hot h;
 };
@@ -191,12 +193,38 @@ __device__ __forceinline__ void launch(Lane &L, Ctx &C, uint32_t id, int batch, 
     load_hot(L.h, C.layer(L, 0));
     L.batch = batch;
     L.events = L.anomalies = L.steps = 0u;
+    L.pending = false;
     L.run_abs = 0ull;
 }
 
-// One hop-drop-spin (or boundary) step plus roulette; returns true when the packet has ended
-// (its per-photon totals are then published).
-template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L, Ctx &C) {
+// Publish an ended packet's per-photon totals (events, anomalies, the weight absorbed in its last
+// layer) into its batch.
+template <class Ctx> __device__ __forceinline__ void finish_photon(const Lane &L, Ctx &C) {
+    C.batch_add(L, 2, static_cast<unsigned long long>(L.events));
+    if (L.anomalies) C.batch_add(L, 3, static_cast<unsigned long long>(L.anomalies));
+    if (L.run_abs) C.batch_add(L, 4 + L.layer, L.run_abs);
+}
+
+// Where an ended packet's totals are published: 0 = at the end of its last step (walk_step);
+// 1 = by the kernel, when the lane takes its next photon or runs out (one warp-uniform place
+// instead of a branch in every step).
+#ifndef TMC_PUBLISH_AT_RELAUNCH
+#define TMC_PUBLISH_AT_RELAUNCH 0
+#endif
+constexpr bool kPublishAtRelaunch = TMC_PUBLISH_AT_RELAUNCH != 0;
+
+// Boundary steps of a warp: 0 = handled in the step that reaches the boundary; K > 0 = a lane that
+// reaches a boundary waits there (the photon's own sequence of operations and random words is
+// unchanged) until at least K lanes of its warp wait, or all of its warp's live lanes do, and they
+// then cross or reflect together (walk_step_deferred).
+#ifndef TMC_DEFER_BOUNDARY
+#define TMC_DEFER_BOUNDARY 0
+#endif
+constexpr int kDeferBoundary = TMC_DEFER_BOUNDARY;
+
+// The first part of a step: refill the random words, the free path (or what is left of it), the
+// distance to the layer's boundary, and the hop. Returns true when the hop ends on the boundary.
+template <int FAST, class Ctx> __device__ __forceinline__ bool step_move(Lane &L, Ctx &C) {
     if constexpr (kRingWords == 8) {
         if (L.wp - L.rp < 4u) C.refill(L);  // a step draws at most 4 words
     } else {
@@ -223,56 +251,61 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
     }
     L.xy = ffma2(f2(s), L.uxy, L.xy);
     L.z = ffma(s, L.uz, L.z);
+    return hit;
+}
 
-    bool died = false;
-    int exit_kind = 0;  // 1: reflectance (top), 2: transmittance (bottom)
-    if (hit) {
-        // ---- boundary: reflect, or transmit into the next layer or out (physics.hpp:198-246)
-        const LayerC &Lc = C.layer(L, L.layer);
-        const bool up = L.uz < 0.0f;
-        const float ca1 = up ? -L.uz : L.uz;
-        const float nt = up ? Lc.n_up : Lc.n_dn;
-        const float rat = up ? Lc.rat_up : Lc.rat_dn;
-        float uz1 = 0.0f;
-        const float r = (ca1 <= (up ? Lc.cc_up : Lc.cc_dn))
-                            ? 1.0f
-                            : fresnel<FAST>(Lc.n, nt, ca1, up ? Lc.rn_up : Lc.rn_dn, rat, uz1);
-        if (unit_open(C.draw(L)) > r) {
-            L.uxy = fmul2(L.uxy, f2(rat));
-            L.uz = up ? -uz1 : uz1;
-            if (up ? L.layer == 0 : L.layer == C.num_layers(L) - 1) {
-                exit_kind = up ? 1 : 2;
-                died = true;
-            } else {
-                if (L.run_abs) {
-                    C.batch_add(L, 4 + L.layer, L.run_abs);
-                    L.run_abs = 0ull;
-                }
-                L.layer += up ? -1 : 1;
-                load_hot(L.h, C.layer(L, L.layer));
-            }
+// At the boundary: reflect, or transmit into the next layer or out (physics.hpp:198-246). Sets
+// exit_kind (1: reflectance, top; 2: transmittance, bottom) and died when the packet leaves.
+template <int FAST, class Ctx>
+__device__ __forceinline__ void step_boundary(Lane &L, Ctx &C, int &exit_kind, bool &died) {
+    const LayerC &Lc = C.layer(L, L.layer);
+    const bool up = L.uz < 0.0f;
+    const float ca1 = up ? -L.uz : L.uz;
+    const float nt = up ? Lc.n_up : Lc.n_dn;
+    const float rat = up ? Lc.rat_up : Lc.rat_dn;
+    float uz1 = 0.0f;
+    const float r = (ca1 <= (up ? Lc.cc_up : Lc.cc_dn)) ? 1.0f
+                                                        : fresnel<FAST>(Lc.n, nt, ca1, up ? Lc.rn_up : Lc.rn_dn, rat, uz1);
+    if (unit_open(C.draw(L)) > r) {
+        L.uxy = fmul2(L.uxy, f2(rat));
+        L.uz = up ? -uz1 : uz1;
+        if (up ? L.layer == 0 : L.layer == C.num_layers(L) - 1) {
+            exit_kind = up ? 1 : 2;
+            died = true;
         } else {
-            L.uz = -L.uz;
+            if (L.run_abs) {
+                C.batch_add(L, 4 + L.layer, L.run_abs);
+                L.run_abs = 0ull;
+            }
+            L.layer += up ? -1 : 1;
+            load_hot(L.h, C.layer(L, L.layer));
         }
     } else {
-        // ---- drop (physics.hpp:187-193) and score the absorption
-        float dwa;
-        if constexpr (Math<FAST>::div) dwa = fmul(L.w, L.h.absorb);
-        else dwa = fmul(L.w, L.h.mua) / L.h.mut;
-        L.w = fsub(L.w, dwa);
-        ++L.events;
-        {
-            const float n2 = norm2(L.uxy, L.uz);
-            if (!(dwa == dwa) || !(fabsf(fsub(n2, 1.0f)) <= 1e-5f)) ++L.anomalies;
-        }
-        const unsigned long long v = to_fixed(dwa);
-        L.run_abs += v;
-        C.absorb(L, v);
-        // ---- spin (physics.hpp:101-144)
-        const float ct = hg_cos<FAST>(L.h, unit_open(C.draw(L)));
-        rotate<FAST>(L.uxy, L.uz, ct, unit_open(C.draw(L)));
+        L.uz = -L.uz;
     }
+}
 
+// An interaction: drop (physics.hpp:187-193), score the absorption, spin (physics.hpp:101-144).
+template <int FAST, class Ctx> __device__ __forceinline__ void step_interaction(Lane &L, Ctx &C) {
+    float dwa;
+    if constexpr (Math<FAST>::div) dwa = fmul(L.w, L.h.absorb);
+    else dwa = fmul(L.w, L.h.mua) / L.h.mut;
+    L.w = fsub(L.w, dwa);
+    ++L.events;
+    {
+        const float n2 = norm2(L.uxy, L.uz);
+        if (!(dwa == dwa) || !(fabsf(fsub(n2, 1.0f)) <= 1e-5f)) ++L.anomalies;
+    }
+    const unsigned long long v = to_fixed(dwa);
+    L.run_abs += v;
+    C.absorb(L, v);
+    const float ct = hg_cos<FAST>(L.h, unit_open(C.draw(L)));
+    rotate<FAST>(L.uxy, L.uz, ct, unit_open(C.draw(L)));
+}
+
+// The end of a step: score an exit, or play roulette (physics.hpp:250-259); the step cap; publish
+// an ended packet (unless the kernel does). Returns true when the packet has ended.
+template <int FAST, class Ctx> __device__ __forceinline__ bool step_tail(Lane &L, Ctx &C, int exit_kind, bool died) {
     if (exit_kind) {
         // ---- score the exit (check, totals, R_d(r,a) or T_t(r,a))
         const float n2 = norm2(L.uxy, L.uz);
@@ -295,12 +328,42 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
         ++L.anomalies;
         died = true;
     }
-    if (died) {
-        C.batch_add(L, 2, static_cast<unsigned long long>(L.events));
-        if (L.anomalies) C.batch_add(L, 3, static_cast<unsigned long long>(L.anomalies));
-        if (L.run_abs) C.batch_add(L, 4 + L.layer, L.run_abs);
+    if constexpr (!kPublishAtRelaunch) {
+        if (died) finish_photon(L, C);
     }
     return died;
+}
+
+// One hop-drop-spin (or boundary) step plus roulette (step_once, physics.hpp:263-277); returns true
+// when the packet has ended (its per-photon totals are then published, here or by the kernel:
+// kPublishAtRelaunch).
+template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L, Ctx &C) {
+    bool died = false;
+    int exit_kind = 0;
+    if (step_move<FAST>(L, C)) step_boundary<FAST>(L, C, exit_kind, died);
+    else step_interaction<FAST>(L, C);
+    return step_tail<FAST>(L, C, exit_kind, died);
+}
+
+// The same step with deferred boundaries (kDeferBoundary > 0): a lane whose hop ends on a
+// boundary marks itself pending and stops there; a pending lane does nothing until the warp says
+// `boundaries` (enough of its lanes are pending), then crosses or reflects and finishes that step.
+// The words drawn and the operations done for each photon are those of walk_step, in its order.
+template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step_deferred(Lane &L, Ctx &C, bool boundaries) {
+    bool died = false;
+    int exit_kind = 0;
+    if (L.pending) {
+        if (!boundaries) return false;
+        L.pending = false;
+        step_boundary<FAST>(L, C, exit_kind, died);
+    } else {
+        if (step_move<FAST>(L, C)) {
+            L.pending = true;
+            return false;
+        }
+        step_interaction<FAST>(L, C);
+    }
+    return step_tail<FAST>(L, C, exit_kind, died);
 }
 
 // The random-word ring: kRingWords words per lane in shared memory, slot k of a block's lanes
