@@ -93,7 +93,8 @@ typedef struct {
     /* Shared-memory tally tiles, for grids whose tallies do not all fit (tmc_b200_plan,
      * tmc_b200_autotune); they change where deposits are summed, never the results. */
     int32_t tile_tz;           /* depth bins of the shared core tile of A(r,z); its radial rows
-                                  follow from the budget. 0 = planner (about 2 sqrt(tile words)) */
+                                  follow from the budget. 0 = planner (about 2 sqrt(tile words)),
+                                  -1 = no core tile (only the cross, if any, in shared memory) */
     int32_t tile_ra_rows;      /* radial rows of R_d(r,a) and of T_t(r,a) kept in shared memory:
                                   0 = planner (an eighth of the budget each), -1 = none */
     int32_t tile_cross;        /* the clamped last row and last column of A(r,z) in shared memory:

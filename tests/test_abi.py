@@ -153,7 +153,7 @@ def test_plan_follows_the_tile_options():
     assert p.tr_rd == p.tr_tt == 10
     p = tmc.plan(skin, tmc.options(batches=100, tile_cross=-1))
     assert p.cross == 0 and p.tr_a * p.tz_a > base.tr_a * base.tz_a
-    for tz in (0, 1, 17, 400):
+    for tz in (-1, 0, 1, 17, 400):
         for rows in (-1, 0, 3, 500):
             for cross in (-1, 0, 1):
                 for bps in (1, 2, 3, 4):
@@ -161,7 +161,9 @@ def test_plan_follows_the_tile_options():
                                  regs_blocks_per_sm=bps)
                     assert q.smem_bytes <= min(232448, 233472 // bps - 1024)
                     assert 0 <= q.tr_a <= 500 and 0 <= q.tz_a <= 400 and 0 <= q.tr_rd <= 500
-    for bad, msg in (({"tile_tz": -1}, "tile_tz"), ({"tile_ra_rows": -2}, "tile_ra_rows"),
+    p = tmc.plan(skin, tmc.options(batches=100, tile_tz=-1))
+    assert p.tr_a == p.tz_a == 0 and p.cross == 1
+    for bad, msg in (({"tile_tz": -2}, "tile_tz"), ({"tile_ra_rows": -2}, "tile_ra_rows"),
                      ({"tile_cross": 2}, "tile_cross")):
         with pytest.raises(tmc.ConfigError, match=msg):
             tmc.plan(skin, tmc.options(batches=100, **bad))

@@ -116,3 +116,25 @@ def test_levenberg_marquardt_recovers_a_known_answer():
     assert (res < 1e-6).all()
     keep = [c for c in range(S.N_FEAT) if c not in (0, 4)]
     np.testing.assert_array_equal(fit[:, keep], start[:, keep])  # fixed features stay put
+
+
+def test_fit_uncertainty_is_calibrated_and_flags_what_the_data_cannot_fix():
+    """lm_uncertainty on the known model: with 1 % noise on the observations the recovered
+    parameters lie within 3 standard errors of the truth in nearly every fit; a parameter the model
+    ignores (feature 1) has no curvature and every fit that frees it is flagged."""
+    rng = np.random.default_rng(7)
+    model = _KnownModel()
+    n = 200
+    truth = np.zeros((n, S.N_FEAT))
+    truth[:, [0, 4]] = rng.uniform(-1, 1, (n, 2))
+    obs = model.predict(truth)[:, :S.N_RD] + rng.normal(0, 0.01, (n, S.N_RD))
+    mask = np.ones((n, S.N_RD))
+    start = truth.copy()
+    start[:, [0, 4]] += rng.uniform(-0.3, 0.3, (n, 2))
+    fit, _ = S.lm_fit(model, start, obs, mask, free=[0, 4], iters=40)
+    se, flag = S.lm_uncertainty(model, fit, obs, mask, [0, 4])
+    assert not flag.any() and np.isfinite(se).all()
+    z = np.abs(fit[:, [0, 4]] - truth[:, [0, 4]]) / se
+    assert (z < 3).mean() > 0.97
+    se2, flag2 = S.lm_uncertainty(model, fit, obs, mask, [0, 1, 4])  # feature 1 does not enter the model
+    assert flag2.all()

@@ -161,7 +161,7 @@ Plan make_plan(const tmc_run_spec &spec, const tmc_options &opt, const DeviceLim
                 p.cross = 1;
                 rem -= cross;
             }
-            if (p.cross || !want_cross) {
+            if (opt.tile_tz >= 0 && (p.cross || !want_cross)) {
                 // the core tile: tz depth bins (about 2 sqrt(words), or as the options say) by as
                 // many radial rows as fit; without the cross it may reach the last row and column
                 const size_t core = rem / 8;
@@ -656,8 +656,8 @@ int tmc_b200_autotune(const tmc_run_spec *spec, tmc_options *opt, uint64_t sampl
             try_opt(o);
         }
         const int tz0 = std::max(1, p0.tz_a);
-        for (int tz : {tz0 / 2, tz0 * 2, tz0 * 4, spec->nz}) {
-            if (tz < 1) continue;
+        for (int tz : {-1, tz0 / 2, tz0 * 2, tz0 * 4, spec->nz}) {
+            if (tz == 0) continue;
             tmc_options o = best;
             o.tile_tz = tz;
             try_opt(o);

@@ -68,7 +68,7 @@ void validate_run(const tmc_run_spec &spec, const tmc_options &opt) {
         fail("threads_per_block must be a multiple of 32 in [32, 256] (0 = planner)");
     if (opt.blocks_per_sm < 0 || opt.blocks_per_sm > 32) fail("blocks_per_sm must be in [0, 32]");
     if (opt.smem_budget < 0) fail("smem_budget must be >= 0");
-    if (opt.tile_tz < 0) fail("tile_tz must be >= 0 (0 = planner)");
+    if (opt.tile_tz < -1) fail("tile_tz must be >= -1 (0 = planner, -1 = no core tile)");
     if (opt.tile_ra_rows < -1) fail("tile_ra_rows must be >= -1 (0 = planner, -1 = none)");
     if (opt.tile_cross < -1 || opt.tile_cross > 1) fail("tile_cross must be -1, 0 or 1");
 }

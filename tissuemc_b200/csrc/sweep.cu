@@ -212,15 +212,15 @@ std::unique_ptr<SweepGraph> build_graph(int cap, int lmax, const tmc_sweep_optio
               static_cast<size_t>(g->threads / 32) * o.tile_r * o.tile_z * 8;
     cudaDeviceProp prop;
     SW_CUDA(cudaGetDeviceProperties(&prop, o.device));
-    SW_CUDA(cudaFuncSetAttribute(sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(g->smem)));
-    SW_CUDA(cudaFuncSetAttribute(sweep_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(g->smem)));
+    // the kernel for these options: fast or exact math, with or without the per-warp tile
+    const bool tile = o.profiles && o.tile_r > 0;
+    const void *kern = o.fast_math ? (tile ? reinterpret_cast<const void *>(sweep_kernel<1, true>)
+                                           : reinterpret_cast<const void *>(sweep_kernel<1, false>))
+                                   : (tile ? reinterpret_cast<const void *>(sweep_kernel<0, true>)
+                                           : reinterpret_cast<const void *>(sweep_kernel<0, false>));
+    SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(g->smem)));
     int bps = 0;
-    if (o.fast_math)
-        SW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, sweep_kernel<1>, g->threads, g->smem));
-    else
-        SW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, sweep_kernel<0>, g->threads, g->smem));
+    SW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, g->threads, g->smem));
     g->grid = prop.multiProcessorCount * std::max(1, bps);
 
     g->off_cfg = align_up(sizeof(SweepHeader));
@@ -270,10 +270,8 @@ std::unique_ptr<SweepGraph> build_graph(int cap, int lmax, const tmc_sweep_optio
         SW_CUDA(cudaMemsetAsync(g->d_tally, 0, g->stride * cap * 8, g->stream));
         SW_CUDA(cudaMemsetAsync(g->d_counter, 0, 256, g->stream));
         SW_CUDA(cudaEventRecordWithFlags(g->e0, g->stream, cudaEventRecordExternal));
-        if (o.fast_math)
-            sweep_kernel<1><<<g->grid, g->threads, g->smem, g->stream>>>(P);
-        else
-            sweep_kernel<0><<<g->grid, g->threads, g->smem, g->stream>>>(P);
+        void *args[] = {&P};
+        SW_CUDA(cudaLaunchKernel(kern, dim3(g->grid), dim3(g->threads), args, g->smem, g->stream));
         SW_CUDA(cudaGetLastError());
         SW_CUDA(cudaEventRecordWithFlags(g->e1, g->stream, cudaEventRecordExternal));
         const int warps_per_block = 8;

@@ -68,9 +68,15 @@ struct SweepParams {
     int tile_r, tile_z;             // per-warp shared tile of A(r,z) (0: none)
 };
 
-constexpr int kNoCacheKey = 0x7FFFFFFF;  // the run cache is empty (tally word indices stay below)
+constexpr int kNoCacheKey = 0x7FFFFFFF;
 
-template <int FAST> struct SweepCtx {
+// 1 (default): a per-lane run cache merges consecutive deposits into one A(r,z) bin; 0: every
+// deposit goes straight to its word
+#ifndef TMC_SWEEP_RUN_CACHE
+#define TMC_SWEEP_RUN_CACHE 1
+#endif  // the run cache is empty (tally word indices stay below)
+
+template <int FAST, bool TILE> struct SweepCtx {
     const SweepParams &P;
     Ring ring;
     uint32_t step_cap;
@@ -90,6 +96,10 @@ template <int FAST> struct SweepCtx {
     uint32_t tile_cfg;
     int tile_t;  // tally offset of tile_cfg
 
+    // the step publishes an ended packet (in the kernel's relaunch it measured slower here: the
+    // sweep kernel is held to 64 registers and spilled)
+    static constexpr bool kPublishAtRelaunch = false;
+
     __device__ __forceinline__ void refill(Lane &L) const { ring.refill(L, sched, static_cast<int>(P.threads)); }
     __device__ __forceinline__ uint32_t draw(Lane &L) const { return ring.draw(L); }
     __device__ __forceinline__ const LayerC &layer(const Lane &, int l) const { return layers[l]; }
@@ -106,8 +116,14 @@ template <int FAST> struct SweepCtx {
         const float rr = radius<FAST>(L.xy);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int iz = bin_of<FAST>(L.z, P.dz, P.inv_dz, P.nz);
-        const int key = (cfg == tile_cfg && ir < P.tile_r && iz < P.tile_z) ? -1 - (ir * P.tile_z + iz)
-                                                                            : t + a_off + ir * P.nz + iz;
+        int key = t + a_off + ir * P.nz + iz;
+        if constexpr (TILE) {
+            if (cfg == tile_cfg && ir < P.tile_r && iz < P.tile_z) key = -1 - (ir * P.tile_z + iz);
+        }
+#if !TMC_SWEEP_RUN_CACHE
+        deposit(key, v);
+        return;
+#endif
         if (key == cache_key) {
             cache_val += v;
         } else {
@@ -160,10 +176,12 @@ template <int FAST> struct SweepCtx {
 #define TMC_SWEEP_BOUNDS __launch_bounds__(256)
 #endif
 
-template <int FAST>
+// TILE: the per-warp shared tile of A(r,z) is on (P.tile_r, P.tile_z > 0); the kernel without it
+// is a separate instantiation, so that the tile's bookkeeping costs nothing when it is off.
+template <int FAST, bool TILE>
 __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParams P) {
     extern __shared__ __align__(16) unsigned long long smem[];
-    SweepCtx<FAST> C{P,
+    SweepCtx<FAST, TILE> C{P,
                      Ring{reinterpret_cast<uint32_t *>(smem) + threadIdx.x, static_cast<int>(P.threads)},
                      P.step_cap,
                      P.nb * (4 + P.lmax),
@@ -186,8 +204,10 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                      0xFFFFFFFFu,
                      0};
     const unsigned lane = threadIdx.x & 31u;
-    for (int i = static_cast<int>(lane); i < P.tile_r * P.tile_z; i += 32) C.tile[i] = 0ull;
-    __syncwarp();
+    if constexpr (TILE) {
+        for (int i = static_cast<int>(lane); i < P.tile_r * P.tile_z; i += 32) C.tile[i] = 0ull;
+        __syncwarp();
+    }
     const unsigned lt_mask = (1u << lane) - 1u;
     const SweepHeader &H = *P.hdr;  // read where an item is taken (rare), not held in registers
 
@@ -196,17 +216,10 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
     bool items_done = false;
     unsigned ex_mask = 0u;  // warp-uniform: lanes with no photon left to take
     bool alive = false;
-    bool held = false;  // L holds a photon whose totals are not yet published (kPublishAtRelaunch)
     Lane L;
 
     for (;;) {
         unsigned need = ~__ballot_sync(0xffffffffu, alive) & ~ex_mask;
-        if constexpr (kPublishAtRelaunch) {
-            if (((need >> lane) & 1u) && held) {  // the lane's last photon ended: publish it
-                finish_photon(L, C);
-                held = false;
-            }
-        }
         while (need) {  // warp-uniform: hand out photons, taking new items as they run out
             const uint32_t avail = it_end - it_next;
             if (avail == 0u) {
@@ -218,7 +231,7 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                     if (idx < H.order.total) {
                         sweep_item(idx, H.order, H.item_photons, H.n_cfg, P.prefix,
                                    [&](uint32_t c) { return P.cfgs[c].photons; }, it_cfg, it_next, it_end);
-                        if (P.tile_r > 0 && it_cfg != C.tile_cfg) {  // the tile follows the warp's item
+                        if (TILE && it_cfg != C.tile_cfg) {  // the tile follows the warp's item
                             C.flush_tile(lane);
                             C.tile_cfg = it_cfg;
                             C.tile_t = static_cast<int>(it_cfg) * P.stride;
@@ -247,26 +260,16 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
                 const int batch = batch_of(id, cf.plan_base, cf.plan_extra, cf.plan_bnd);
                 launch(L, C, id, batch, cf.launch_w);
                 alive = true;
-                held = true;
             }
             need &= ~__ballot_sync(0xffffffffu, mine);
             it_next += take;
         }
         if (ex_mask == 0xffffffffu) break;  // exhausted lanes hold no photon: the warp is done
-        if constexpr (kDeferBoundary > 0) {
-            // lanes waiting on a boundary cross together once enough of them (or all) wait
-            const unsigned live = __ballot_sync(0xffffffffu, alive);
-            const unsigned pend = __ballot_sync(0xffffffffu, alive && L.pending);
-            const bool boundaries = pend != 0u && (__popc(pend) >= kDeferBoundary || pend == live);
-            if (!alive) continue;
-            if (walk_step_deferred<FAST>(L, C, boundaries)) alive = false;
-        } else {
-            if (!alive) continue;
-            if (walk_step<FAST>(L, C)) alive = false;
-        }
+        if (!alive) continue;
+        if (walk_step<FAST>(L, C)) alive = false;
     }
     C.flush_cache();
-    if (P.tile_r > 0) C.flush_tile(lane);
+    if constexpr (TILE) C.flush_tile(lane);
 }
 
 // Per-configuration summaries from the integer tallies, in double: R_d(r) per photon (nr values,

@@ -27,18 +27,19 @@ constexpr float kFixedScale = 4294967296.0f;  // 2^32
 constexpr uint32_t kDefaultStepCap = 2000000000u;  // steps after which a live packet is an anomaly
 
 // Constants of one layer, computed on the host in float arithmetic in the same order as the
-// reference evaluates them (so e.g. hg_a is exactly float(1) - g * g).
-struct LayerC {
-    float mua, mus, mut, inv_mut;     // mut = mua + mus
-    float absorb;                     // mua / mut
-    float z0, z1;                     // top and bottom depth [cm]
-    float g, hg_a, hg_b, hg_c, hg_d;  // 1 - g*g, 1 - g, 2*g, 1 + g*g
-    float inv_2g;                     // 1 / (2*g), 0 when g == 0
-    float n, n_up, n_dn;              // this layer's index and its neighbours' (ambient at the ends)
-    float cc_up, cc_dn;               // critical cosines toward the top and the bottom (0 if none)
-    float rat_up, rat_dn;             // n / n_up, n / n_dn
-    float rn_up, rn_dn;               // normal-incidence Fresnel reflectance toward each side
-    float pad[2];
+// reference evaluates them (so e.g. hg_a is exactly float(1) - g * g). Laid out as six 16-byte
+// groups: the first three are what a packet keeps in registers while it is in the layer (three
+// 16-byte loads on entering it); the next two describe the boundary toward each side (one 16-byte
+// load for the side a packet meets).
+struct __align__(16) LayerC {
+    float inv_mut, absorb, z0, z1;    // 1 / mu_t, mu_a / mu_t, top and bottom depth [cm]
+    float g, hg_a, hg_b, hg_c;        // g, 1 - g*g, 1 - g, 2*g
+    float hg_d, inv_2g, mut, mua;     // 1 + g*g, 1 / (2*g) (0 when g == 0), mu_a + mu_s, mu_a
+    float n_up, rat_up, cc_up, rn_up; // toward the top: the neighbour's index (ambient at the end),
+                                      // n / n_up, the critical cosine (0 if none), the
+                                      // normal-incidence Fresnel reflectance
+    float n_dn, rat_dn, cc_dn, rn_dn; // the same toward the bottom
+    float n, mus, pad[2];             // this layer's index, mu_s
 };
 static_assert(sizeof(LayerC) == 24 * 4, "LayerC layout");
 

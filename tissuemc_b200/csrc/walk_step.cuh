@@ -13,6 +13,8 @@
 //   ctx.exit(lane, kind, v)   score an exit (1: reflectance, 2: transmittance) of v
 //   ctx.batch_add(lane, i, v) add v to slot i of the lane's batch totals
 //   ctx.step_cap              steps after which a packet is ended as an anomaly
+//   Ctx::kPublishAtRelaunch   true: the kernel publishes an ended packet's totals (finish_photon)
+//                             when the lane relaunches; false: the step does
 #pragma once
 
 #include "walk.cuh"
@@ -29,6 +31,14 @@ namespace tmc {
 #define TMC_RING_WORDS 16
 #endif
 constexpr uint32_t kRingWords = TMC_RING_WORDS;
+
+// Where a packet keeps its layer's hot constants (Hot): 0 = in registers, loaded on entering a
+// layer; 1 = read from the layer table (shared memory, three 16-byte loads) at every step, which
+// frees twelve registers per lane for more resident warps.
+#ifndef TMC_HOT_SMEM
+#define TMC_HOT_SMEM 0
+#endif
+constexpr bool kHotInSmem = TMC_HOT_SMEM != 0;
 static_assert(kRingWords == 8 || kRingWords == 16, "ring of 8 or 16 words");
 
 constexpr float kCosZero = 1.0f - 1e-6f;  // physics.hpp:35 (float widening of MCML COSZERO)
@@ -43,18 +53,26 @@ struct Hot {
 };
 
 __device__ __forceinline__ void load_hot(Hot &h, const LayerC &L) {
-    h.mua = L.mua;
-    h.mut = L.mut;
-    h.inv_mut = L.inv_mut;
-    h.absorb = L.absorb;
-    h.z0 = L.z0;
-    h.z1 = L.z1;
-    h.g = L.g;
-    h.hg_a = L.hg_a;
-    h.hg_b = L.hg_b;
-    h.hg_c = L.hg_c;
-    h.hg_d = L.hg_d;
-    h.inv_2g = L.inv_2g;
+    const float4 *q = reinterpret_cast<const float4 *>(&L);  // three 16-byte loads
+    const float4 a = q[0], b = q[1], c = q[2];
+    h.inv_mut = a.x;
+    h.absorb = a.y;
+    h.z0 = a.z;
+    h.z1 = a.w;
+    h.g = b.x;
+    h.hg_a = b.y;
+    h.hg_b = b.z;
+    h.hg_c = b.w;
+    h.hg_d = c.x;
+    h.inv_2g = c.y;
+    h.mut = c.z;
+    h.mua = c.w;
+}
+
+// The boundary of layer L toward the top (up) or the bottom: the neighbour's index, the index
+// ratio, the critical cosine and the normal-incidence reflectance, in one 16-byte load.
+__device__ __forceinline__ float4 boundary_side(const LayerC &L, bool up) {
+    return reinterpret_cast<const float4 *>(&L)[up ? 3 : 4];
 }
 
 // Fresnel reflectance for unpolarised light from index n1 into n2 at cos(incidence) ca1
@@ -172,7 +190,6 @@ struct Lane {
     int layer, batch;
     uint32_t id, blk, rp, wp;  // photon id, Philox block, ring read/write positions
     uint32_t events, anomalies, steps;
-    bool pending;                // stopped on a boundary, waiting for its warp (kDeferBoundary)
     unsigned long long run_abs;  // fixed-point weight absorbed in the current layer
     Hot h;
 };
@@ -190,10 +207,9 @@ __device__ __forceinline__ void launch(Lane &L, Ctx &C, uint32_t id, int batch, 
     L.w = launch_w;
     L.sleft = 0.f;
     L.layer = 0;
-    load_hot(L.h, C.layer(L, 0));
+    if constexpr (!kHotInSmem) load_hot(L.h, C.layer(L, 0));
     L.batch = batch;
     L.events = L.anomalies = L.steps = 0u;
-    L.pending = false;
     L.run_abs = 0ull;
 }
 
@@ -205,26 +221,20 @@ template <class Ctx> __device__ __forceinline__ void finish_photon(const Lane &L
     if (L.run_abs) C.batch_add(L, 4 + L.layer, L.run_abs);
 }
 
-// Where an ended packet's totals are published: 0 = at the end of its last step (walk_step);
-// 1 = by the kernel, when the lane takes its next photon or runs out (one warp-uniform place
-// instead of a branch in every step).
-#ifndef TMC_PUBLISH_AT_RELAUNCH
-#define TMC_PUBLISH_AT_RELAUNCH 0
-#endif
-constexpr bool kPublishAtRelaunch = TMC_PUBLISH_AT_RELAUNCH != 0;
-
-// Boundary steps of a warp: 0 = handled in the step that reaches the boundary; K > 0 = a lane that
-// reaches a boundary waits there (the photon's own sequence of operations and random words is
-// unchanged) until at least K lanes of its warp wait, or all of its warp's live lanes do, and they
-// then cross or reflect together (walk_step_deferred).
-#ifndef TMC_DEFER_BOUNDARY
-#define TMC_DEFER_BOUNDARY 0
-#endif
-constexpr int kDeferBoundary = TMC_DEFER_BOUNDARY;
-
 // The first part of a step: refill the random words, the free path (or what is left of it), the
 // distance to the layer's boundary, and the hop. Returns true when the hop ends on the boundary.
-template <int FAST, class Ctx> __device__ __forceinline__ bool step_move(Lane &L, Ctx &C) {
+// The layer constants of the packet's current layer (registers, or the layer table: kHotInSmem).
+template <class Ctx> __device__ __forceinline__ Hot hot_of(const Lane &L, Ctx &C) {
+    if constexpr (kHotInSmem) {
+        Hot h;
+        load_hot(h, C.layer(L, L.layer));
+        return h;
+    } else {
+        return L.h;
+    }
+}
+
+template <int FAST, class Ctx> __device__ __forceinline__ bool step_move(Lane &L, Ctx &C, const Hot &h) {
     if constexpr (kRingWords == 8) {
         if (L.wp - L.rp < 4u) C.refill(L);  // a step draws at most 4 words
     } else {
@@ -234,17 +244,17 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool step_move(Lane &L
     ++L.steps;
     float s;
     if (L.sleft == 0.0f) {
-        s = step_length<FAST>(L.h, unit_open(C.draw(L)));
+        s = step_length<FAST>(h, unit_open(C.draw(L)));
     } else {
-        if constexpr (Math<FAST>::div) s = fmul(L.sleft, L.h.inv_mut);
-        else s = L.sleft / L.h.mut;
+        if constexpr (Math<FAST>::div) s = fmul(L.sleft, h.inv_mut);
+        else s = L.sleft / h.mut;
         L.sleft = 0.0f;
     }
     bool hit = false;
     if (L.uz != 0.0f) {
-        const float db = m_div<FAST>(fsub(L.uz > 0.0f ? L.h.z1 : L.h.z0, L.z), L.uz);
+        const float db = m_div<FAST>(fsub(L.uz > 0.0f ? h.z1 : h.z0, L.z), L.uz);
         if (s > db) {
-            L.sleft = fmul(fsub(s, db), L.h.mut);
+            L.sleft = fmul(fsub(s, db), h.mut);
             s = db;
             hit = true;
         }
@@ -261,11 +271,10 @@ __device__ __forceinline__ void step_boundary(Lane &L, Ctx &C, int &exit_kind, b
     const LayerC &Lc = C.layer(L, L.layer);
     const bool up = L.uz < 0.0f;
     const float ca1 = up ? -L.uz : L.uz;
-    const float nt = up ? Lc.n_up : Lc.n_dn;
-    const float rat = up ? Lc.rat_up : Lc.rat_dn;
+    const float4 side = boundary_side(Lc, up);  // n_t, n / n_t, critical cosine, normal-incidence R
+    const float nt = side.x, rat = side.y;
     float uz1 = 0.0f;
-    const float r = (ca1 <= (up ? Lc.cc_up : Lc.cc_dn)) ? 1.0f
-                                                        : fresnel<FAST>(Lc.n, nt, ca1, up ? Lc.rn_up : Lc.rn_dn, rat, uz1);
+    const float r = (ca1 <= side.z) ? 1.0f : fresnel<FAST>(Lc.n, nt, ca1, side.w, rat, uz1);
     if (unit_open(C.draw(L)) > r) {
         L.uxy = fmul2(L.uxy, f2(rat));
         L.uz = up ? -uz1 : uz1;
@@ -278,7 +287,7 @@ __device__ __forceinline__ void step_boundary(Lane &L, Ctx &C, int &exit_kind, b
                 L.run_abs = 0ull;
             }
             L.layer += up ? -1 : 1;
-            load_hot(L.h, C.layer(L, L.layer));
+            if constexpr (!kHotInSmem) load_hot(L.h, C.layer(L, L.layer));
         }
     } else {
         L.uz = -L.uz;
@@ -286,10 +295,10 @@ __device__ __forceinline__ void step_boundary(Lane &L, Ctx &C, int &exit_kind, b
 }
 
 // An interaction: drop (physics.hpp:187-193), score the absorption, spin (physics.hpp:101-144).
-template <int FAST, class Ctx> __device__ __forceinline__ void step_interaction(Lane &L, Ctx &C) {
+template <int FAST, class Ctx> __device__ __forceinline__ void step_interaction(Lane &L, Ctx &C, const Hot &h) {
     float dwa;
-    if constexpr (Math<FAST>::div) dwa = fmul(L.w, L.h.absorb);
-    else dwa = fmul(L.w, L.h.mua) / L.h.mut;
+    if constexpr (Math<FAST>::div) dwa = fmul(L.w, h.absorb);
+    else dwa = fmul(L.w, h.mua) / h.mut;
     L.w = fsub(L.w, dwa);
     ++L.events;
     {
@@ -299,12 +308,13 @@ template <int FAST, class Ctx> __device__ __forceinline__ void step_interaction(
     const unsigned long long v = to_fixed(dwa);
     L.run_abs += v;
     C.absorb(L, v);
-    const float ct = hg_cos<FAST>(L.h, unit_open(C.draw(L)));
+    const float ct = hg_cos<FAST>(h, unit_open(C.draw(L)));
     rotate<FAST>(L.uxy, L.uz, ct, unit_open(C.draw(L)));
 }
 
 // The end of a step: score an exit, or play roulette (physics.hpp:250-259); the step cap; publish
-// an ended packet (unless the kernel does). Returns true when the packet has ended.
+// an ended packet (unless the kernel does: Ctx::kPublishAtRelaunch). Returns true when the packet
+// has ended.
 template <int FAST, class Ctx> __device__ __forceinline__ bool step_tail(Lane &L, Ctx &C, int exit_kind, bool died) {
     if (exit_kind) {
         // ---- score the exit (check, totals, R_d(r,a) or T_t(r,a))
@@ -328,41 +338,22 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool step_tail(Lane &L
         ++L.anomalies;
         died = true;
     }
-    if constexpr (!kPublishAtRelaunch) {
+    if constexpr (!Ctx::kPublishAtRelaunch) {
         if (died) finish_photon(L, C);
     }
     return died;
 }
 
 // One hop-drop-spin (or boundary) step plus roulette (step_once, physics.hpp:263-277); returns true
-// when the packet has ended (its per-photon totals are then published, here or by the kernel:
-// kPublishAtRelaunch).
+// when the packet has ended. Its per-photon totals are then published here, or, when the context
+// says Ctx::kPublishAtRelaunch, by the kernel when the lane takes its next photon or runs out (one
+// warp-uniform place instead of a branch in every step).
 template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L, Ctx &C) {
     bool died = false;
     int exit_kind = 0;
-    if (step_move<FAST>(L, C)) step_boundary<FAST>(L, C, exit_kind, died);
-    else step_interaction<FAST>(L, C);
-    return step_tail<FAST>(L, C, exit_kind, died);
-}
-
-// The same step with deferred boundaries (kDeferBoundary > 0): a lane whose hop ends on a
-// boundary marks itself pending and stops there; a pending lane does nothing until the warp says
-// `boundaries` (enough of its lanes are pending), then crosses or reflects and finishes that step.
-// The words drawn and the operations done for each photon are those of walk_step, in its order.
-template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step_deferred(Lane &L, Ctx &C, bool boundaries) {
-    bool died = false;
-    int exit_kind = 0;
-    if (L.pending) {
-        if (!boundaries) return false;
-        L.pending = false;
-        step_boundary<FAST>(L, C, exit_kind, died);
-    } else {
-        if (step_move<FAST>(L, C)) {
-            L.pending = true;
-            return false;
-        }
-        step_interaction<FAST>(L, C);
-    }
+    const Hot h = hot_of(L, C);
+    if (step_move<FAST>(L, C, h)) step_boundary<FAST>(L, C, exit_kind, died);
+    else step_interaction<FAST>(L, C, h);
     return step_tail<FAST>(L, C, exit_kind, died);
 }
 

@@ -613,6 +613,36 @@ def lm_fit(ens: Ensemble, base_feats: np.ndarray, obs_log_rd: np.ndarray, mask: 
     return theta, np.sqrt(cost)
 
 
+def lm_uncertainty(ens, theta: np.ndarray, obs_log_rd: np.ndarray, mask: np.ndarray, free: list[int],
+                   h: float = 0.03, max_se: float = 0.25) -> tuple[np.ndarray, np.ndarray]:
+    """Per-parameter standard errors of fitted features, from the surrogate's Jacobian at the fit:
+    cov = s^2 (J^T J)^-1 with s^2 the residual variance over the fitted bins (m bins, p parameters,
+    s^2 = |r|^2 / (m - p)). A fit is flagged unidentifiable when a parameter's standard error
+    exceeds max_se (log10 units; 0.25 is a factor of 1.8) or J^T J is singular: the data then do
+    not pin that parameter down, whatever value the fit returned. Returns (se: n x p, flag: n)."""
+    n, p = len(theta), len(free)
+    pert = np.repeat(theta[None], 2 * p + 1, 0)
+    for j, col in enumerate(free):
+        pert[2 * j, :, col] += h
+        pert[2 * j + 1, :, col] -= h
+    y = ens.predict(pert.reshape(-1, theta.shape[1])).reshape(2 * p + 1, n, -1)[..., :N_RD]
+    J = np.stack([(y[2 * j] - y[2 * j + 1]) / (2 * h) * mask for j in range(p)], axis=2)
+    r = (y[2 * p] - obs_log_rd) * mask
+    m = np.maximum(mask.sum(-1) if mask.ndim > 1 else np.full(n, mask.sum()), p + 1)
+    s2 = (r ** 2).sum(1) / (m - p)
+    JtJ = np.einsum("nbi,nbj->nij", J, J)
+    se = np.full((n, p), np.inf)
+    flag = np.ones(n, dtype=bool)
+    for i in range(n):
+        w = np.linalg.eigvalsh(JtJ[i])
+        if w.min() <= 1e-12 * max(w.max(), 1e-300):
+            continue
+        cov = s2[i] * np.linalg.inv(JtJ[i])
+        se[i] = np.sqrt(np.maximum(np.diagonal(cov), 0.0))
+        flag[i] = bool((se[i] > max_se).any())
+    return se, flag
+
+
 def config_from_features(f: np.ndarray, photons: int, seed: int) -> CSweepConfig:
     """A sweep configuration from a raw feature vector (inverse of `features`)."""
     c = CSweepConfig()
@@ -635,7 +665,7 @@ def pipeline(scale: float = 1.0, members: int = 4, epochs: int = 300, seed: int 
     """Train, evaluate and serve the surrogate end to end; returns the measurements.
 
     Full size (scale 1): 2^20 training and 2^16 held-out solves at 1e5 photons from the batched
-    sweep; accuracy on 64 held-out configurations against 1e8-photon Monte Carlo (bins with at
+    sweep; accuracy on 256 held-out configurations against 1e8-photon Monte Carlo (bins with at
     least 1e4 photons' worth of signal, i.e. R_d(r) * area * 1e8 >= 1e4); 1e6 gated queries in
     batches of 65,536 (queries whose members' R_d disagree by more than 1 % go back to plain Monte
     Carlo at 1e6 photons, one batched sweep); 1024 inverse fits of (mu_a, mu_s') of both layers of
@@ -669,7 +699,7 @@ def pipeline(scale: float = 1.0, members: int = 4, epochs: int = 300, seed: int 
     log(f"train: {out['train']}, held-out normalised MSE {out['held_out_mse_normalised']:.4f}")
 
     # accuracy against high-photon Monte Carlo
-    n_acc = max(8, int(64 * min(1.0, scale * 4)))
+    n_acc = max(8, int(256 * min(1.0, scale * 4)))
     acc_photons = 100_000_000 if scale >= 0.25 else 10_000_000
     acc_cfgs = (CSweepConfig * n_acc)(*hcfg[:n_acc])
     for c in acc_cfgs:
@@ -782,9 +812,24 @@ def pipeline(scale: float = 1.0, members: int = 4, epochs: int = 300, seed: int 
     v_log = np.log10(np.maximum(vsum[:, :N_RD] / areas, RD_FLOOR))
     v_rms = np.sqrt((((v_log - obs_log) * mask) ** 2).sum(1) / np.maximum(mask.sum(1), 1))
     err = np.abs(fit[:, free] - truth[:, free])
-    out["inverse_fit"] = {"fits": len(two), "seconds": t_fit, "median_abs_log10_err": [float(np.median(err[:, j]))
-                                                                                        for j in range(4)],
-                          "verified_rms_log10_residual_median": float(np.median(v_rms)),
-                          "verified_within_5pct": float((v_rms < np.log10(1.05)).mean())}
+    se, flagged = lm_uncertainty(ens, fit, obs_log, mask, free)
+    ok = ~flagged
+    names = ["log10 mua1", "log10 mus'1", "log10 mua2", "log10 mus'2"]
+    out["inverse_fit"] = {
+        "fits": len(two), "seconds": t_fit,
+        "median_abs_log10_err": [float(np.median(err[:, j])) for j in range(4)],
+        "p90_abs_log10_err": [float(np.quantile(err[:, j], 0.9)) for j in range(4)],
+        "parameters": names,
+        # per-parameter standard errors from the surrogate's Jacobian at the fit; a fit whose
+        # standard error exceeds 0.25 (log10) in any parameter is flagged as not identified
+        "median_se_log10": [float(np.median(se[np.isfinite(se[:, j]), j])) if np.isfinite(se[:, j]).any() else None
+                            for j in range(4)],
+        "flagged_unidentifiable": float(flagged.mean()),
+        "identified_median_abs_log10_err": [float(np.median(err[ok, j])) if ok.any() else None for j in range(4)],
+        "flagged_median_abs_log10_err": [float(np.median(err[flagged, j])) if flagged.any() else None
+                                         for j in range(4)],
+        "within_2se": [float((err[ok, j] <= 2 * se[ok, j]).mean()) if ok.any() else None for j in range(4)],
+        "verified_rms_log10_residual_median": float(np.median(v_rms)),
+        "verified_within_5pct": float((v_rms < np.log10(1.05)).mean())}
     log(f"inverse fit: {out['inverse_fit']}")
     return out
