@@ -96,8 +96,8 @@ template <int FAST> struct PlainCtx {
     __device__ __forceinline__ void absorb(const Lane &L, unsigned long long v) const {
         if (!P.profiles) return;
         const float rr = radius<FAST>(L.xy);
-        const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
-        const int iz = bin_of<FAST>(L.z, P.dz, P.inv_dz, P.nz);
+        int ir, iz;
+        bins_rz<FAST>(rr, L.z, P.dr, P.dz, P.inv_dr, P.inv_dz, P.nr, P.nz, ir, iz);
         deposit(ir, iz, v);
     }
 

@@ -108,11 +108,30 @@ __device__ __forceinline__ float fresnel(float n1, float n2, float ca1, float rn
 
 // Clamped bin index (src/cpu/engine.cpp:59-66 semantics, branch-free): x <= 0 or NaN -> 0,
 // x / width >= n -> n - 1, else floor(x / width).
+// The clamp is the conversion's own: a float-to-unsigned conversion that truncates turns negative
+// values and NaN into 0 and saturates large ones, so min(u, n - 1) is the clamped bin.
+__device__ __forceinline__ int clamp_bin(float i, int n) {
+    return static_cast<int>(umin(__float2uint_rz(i), static_cast<unsigned>(n - 1)));
+}
 template <int FAST> __device__ __forceinline__ int bin_of(float x, float width, float inv_width, int n) {
     float i;
     if constexpr (Math<FAST>::div) i = fmul(x, inv_width);
     else i = x / width;
-    return static_cast<int>(fminf(fmaxf(i, 0.0f), static_cast<float>(n - 1)));
+    return clamp_bin(i, n);
+}
+// The radius and depth bins of one deposit (r, z) together: in fast math the two products are one
+// paired instruction.
+template <int FAST>
+__device__ __forceinline__ void bins_rz(float r, float z, float dr, float dz, float inv_dr, float inv_dz, int nr, int nz,
+                                        int &ir, int &iz) {
+    if constexpr (Math<FAST>::div) {
+        const float2 i = fmul2(f2(r, z), f2(inv_dr, inv_dz));
+        ir = clamp_bin(i.x, nr);
+        iz = clamp_bin(i.y, nz);
+    } else {
+        ir = bin_of<FAST>(r, dr, inv_dr, nr);
+        iz = bin_of<FAST>(z, dz, inv_dz, nz);
+    }
 }
 
 // Free path -ln(u) / mu_t of an interaction step (physics.hpp:148-158).
@@ -302,8 +321,9 @@ template <int FAST, class Ctx> __device__ __forceinline__ void step_interaction(
     L.w = fsub(L.w, dwa);
     ++L.events;
     {
+        // a NaN weight turns the norm's deviation into NaN (0 * NaN), which fails the comparison
         const float n2 = norm2(L.uxy, L.uz);
-        if (!(dwa == dwa) || !(fabsf(fsub(n2, 1.0f)) <= 1e-5f)) ++L.anomalies;
+        if (!(fabsf(ffma(dwa, 0.0f, fsub(n2, 1.0f))) <= 1e-5f)) ++L.anomalies;
     }
     const unsigned long long v = to_fixed(dwa);
     L.run_abs += v;
