@@ -103,6 +103,7 @@ template <int FAST, bool TILE> struct SweepCtx {
 
     __device__ __forceinline__ void refill(Lane &L) const { ring.refill(L, sched, static_cast<int>(P.threads)); }
     __device__ __forceinline__ uint32_t draw(Lane &L) const { return ring.draw(L); }
+    __device__ __forceinline__ void skip(Lane &L) const { ring.skip(L); }
     __device__ __forceinline__ const LayerC &layer(const Lane &, int l) const { return layers[l]; }
     __device__ __forceinline__ int num_layers(const Lane &) const { return nl; }
     __device__ __forceinline__ void batch_add(const Lane &L, int slot, unsigned long long v) const {
@@ -183,7 +184,7 @@ template <int FAST, bool TILE>
 __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParams P) {
     extern __shared__ __align__(16) unsigned long long smem[];
     SweepCtx<FAST, TILE> C{P,
-                     Ring{reinterpret_cast<uint32_t *>(smem) + threadIdx.x, static_cast<int>(P.threads)},
+                     Ring{reinterpret_cast<uint32_t *>(smem) + ring_lane_offset(), static_cast<int>(P.threads)},
                      P.step_cap,
                      P.nb * (4 + P.lmax),
                      P.nb * (4 + P.lmax) + P.nr * P.nz,

@@ -62,6 +62,7 @@ template <int FAST> struct PlainCtx {
 
     __device__ __forceinline__ void refill(Lane &L) const { ring.refill(L, P.round_keys); }
     __device__ __forceinline__ uint32_t draw(Lane &L) const { return ring.draw(L); }
+    __device__ __forceinline__ void skip(Lane &L) const { ring.skip(L); }
     __device__ __forceinline__ const LayerC &layer(const Lane &, int l) const { return layers[l]; }
     __device__ __forceinline__ int num_layers(const Lane &) const { return P.nl; }
     __device__ __forceinline__ void batch_add(const Lane &L, int slot, unsigned long long v) const {
@@ -139,7 +140,7 @@ __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P
     }
     __syncthreads();
     PlainCtx<FAST> C{P,
-                     Ring{reinterpret_cast<uint32_t *>(smem + S.ring) + threadIdx.x, static_cast<int>(P.threads)},
+                     Ring{reinterpret_cast<uint32_t *>(smem + S.ring) + ring_lane_offset(), static_cast<int>(P.threads)},
                      P.step_cap,
                      reinterpret_cast<const LayerC *>(smem + S.layers),
                      P.batch_smem ? smem + S.batch : P.g_batch,

@@ -293,8 +293,23 @@ __device__ __forceinline__ void step_boundary(Lane &L, Ctx &C, int &exit_kind, b
     const float4 side = boundary_side(Lc, up);  // n_t, n / n_t, critical cosine, normal-incidence R
     const float nt = side.x, rat = side.y;
     float uz1 = 0.0f;
+#if TMC_MATCHED_FAST
+    bool through;
+    if (nt == Lc.n) {
+        // matched indices: R = 0, so the Fresnel word (in (0, 1), always above R) is drawn and not
+        // needed, and the direction goes through unchanged (rat = 1, cos_t = cos_i)
+        C.skip(L);
+        through = true;
+        uz1 = ca1;
+    } else {
+        const float r = (ca1 <= side.z) ? 1.0f : fresnel<FAST>(Lc.n, nt, ca1, side.w, rat, uz1);
+        through = unit_open(C.draw(L)) > r;
+    }
+    if (through) {
+#else
     const float r = (ca1 <= side.z) ? 1.0f : fresnel<FAST>(Lc.n, nt, ca1, side.w, rat, uz1);
     if (unit_open(C.draw(L)) > r) {
+#endif
         L.uxy = fmul2(L.uxy, f2(rat));
         L.uz = up ? -uz1 : uz1;
         if (up ? L.layer == 0 : L.layer == C.num_layers(L) - 1) {
@@ -377,24 +392,42 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
     return step_tail<FAST>(L, C, exit_kind, died);
 }
 
-// The random-word ring: kRingWords words per lane in shared memory, slot k of a block's lanes
-// contiguous (ring[k * stride]), so lanes reading different slots never conflict on a bank.
+// This lane's slot 0 in its block's ring area: slot k of a block's lanes contiguous (ring[k * stride],
+// stride = the block's threads), or with TMC_RING_PER_WARP slot k of a warp's 32 lanes contiguous in
+// the warp's own region; either way the lanes of a warp never conflict on a bank.
+__device__ __forceinline__ int ring_lane_offset() {
+#if TMC_RING_PER_WARP
+    return static_cast<int>((threadIdx.x >> 5) * (kRingWords * 32u) + (threadIdx.x & 31u));
+#else
+    return static_cast<int>(threadIdx.x);
+#endif
+}
+
+// The random-word ring: kRingWords words per lane in shared memory.
 struct Ring {
     uint32_t *base;  // this lane's slot 0
     int stride;      // lanes per block
 
     __device__ __forceinline__ uint32_t draw(Lane &L) const {
-        const uint32_t o = base[(L.rp & (kRingWords - 1u)) * stride];
+        const uint32_t o = base[(L.rp & (kRingWords - 1u)) * slot_stride()];
         ++L.rp;
         return o;
     }
+    // pass over the next word without reading it
+    __device__ __forceinline__ void skip(Lane &L) const { ++L.rp; }
+#if TMC_RING_PER_WARP
+    // each warp's ring is its own region: slot k of its 32 lanes at k * 32 words
+    __device__ __forceinline__ static constexpr int slot_stride() { return 32; }
+#else
+    __device__ __forceinline__ int slot_stride() const { return stride; }
+#endif
     __device__ __forceinline__ void store(Lane &L, uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3) const {
         ++L.blk;
-        uint32_t *const slot = base + (L.wp & (kRingWords - 4u)) * stride;  // wp is a multiple of 4
+        uint32_t *const slot = base + (L.wp & (kRingWords - 4u)) * slot_stride();  // wp is a multiple of 4
         slot[0] = b0;
-        slot[stride] = b1;
-        slot[2 * stride] = b2;
-        slot[3 * stride] = b3;
+        slot[slot_stride()] = b1;
+        slot[2 * slot_stride()] = b2;
+        slot[3 * slot_stride()] = b3;
         L.wp += 4u;
     }
     __device__ __forceinline__ void refill(Lane &L, uint32_t k0, uint32_t k1) const {
