@@ -310,9 +310,10 @@ TMC_B200_API int tmc_b200_sweep_run(const tmc_sweep_config *cfgs, int32_t n, con
 TMC_B200_API int tmc_b200_sweep_run_loop(const tmc_sweep_config *cfgs, int32_t n, const tmc_sweep_options *opt,
                                          uint64_t *raw, double *seconds, tmc_status *status);
 
-/* Autotune the sweep's launch shape on these configurations: block size {128, 256} x photons per
- * work item {64, 256, 1024}, then the per-warp shared tile of A(r,z) {none, 8 x 8, 16 x 16,
- * 16 x 32} with the best of those, each timed on a second run; writes the fastest into *opt. */
+/* Autotune the sweep's launch shape on these configurations: the caller's options, then block size
+ * {128, 256} x photons per work item {64, 256, 1024}, then the per-warp shared tile of A(r,z)
+ * {8 x 8, 16 x 16, 16 x 32} with the best of those, each timed on a second run; a candidate
+ * replaces the best so far only when it is at least 1.5 % faster. Writes the choice into *opt. */
 TMC_B200_API int tmc_b200_sweep_autotune(const tmc_sweep_config *cfgs, int32_t n, tmc_sweep_options *opt,
                                          double *best_seconds, tmc_status *status);
 

