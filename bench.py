@@ -299,15 +299,13 @@ def measure_sweep(configs: int, steps: int, warmup: int, device: int, seed: int 
     opt = tmc.sweep_options(device=device)
     tuned = None
     if autotune:
-        # the launch shape and per-warp tile, timed on the same configurations at a third of their
-        # photons (tmc_b200_sweep_autotune); the results do not depend on them
-        sample = (tmc.CSweepConfig * len(cfgs))()
-        for i, c in enumerate(cfgs):
-            sample[i] = c
-            sample[i].photons = max(int(opt.batches), int(c.photons) // 3)
+        # the launch shape and per-warp tile, timed on this sweep itself (tmc_b200_sweep_autotune;
+        # samples of fewer photons picked shapes that were slower at full size); the results do not
+        # depend on them
+        sample = cfgs
         t_default = min(tmc.sweep_run(sample, opt).seconds for _ in range(2))
         opt, t_best = tmc.sweep_autotune(sample, opt)
-        tuned = {"sample": "the same configurations at a third of their photons",
+        tuned = {"sample": "the workload itself",
                  "sample_seconds_default": t_default, "sample_seconds_chosen": t_best,
                  "options": {k: int(getattr(opt, k)) for k in ("threads_per_block", "item_photons", "tile_r",
                                                                 "tile_z")}}

@@ -104,6 +104,7 @@ template <int FAST, bool TILE> struct SweepCtx {
     __device__ __forceinline__ void refill(Lane &L) const { ring.refill(L, sched, static_cast<int>(P.threads)); }
     __device__ __forceinline__ uint32_t draw(Lane &L) const { return ring.draw(L); }
     __device__ __forceinline__ void skip(Lane &L) const { ring.skip(L); }
+    __device__ __forceinline__ uint32_t peek(const Lane &L) const { return ring.peek(L); }
     __device__ __forceinline__ const LayerC &layer(const Lane &, int l) const { return layers[l]; }
     __device__ __forceinline__ int num_layers(const Lane &) const { return nl; }
     __device__ __forceinline__ void batch_add(const Lane &L, int slot, unsigned long long v) const {

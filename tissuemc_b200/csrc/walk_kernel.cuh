@@ -63,6 +63,7 @@ template <int FAST> struct PlainCtx {
     __device__ __forceinline__ void refill(Lane &L) const { ring.refill(L, P.round_keys); }
     __device__ __forceinline__ uint32_t draw(Lane &L) const { return ring.draw(L); }
     __device__ __forceinline__ void skip(Lane &L) const { ring.skip(L); }
+    __device__ __forceinline__ uint32_t peek(const Lane &L) const { return ring.peek(L); }
     __device__ __forceinline__ const LayerC &layer(const Lane &, int l) const { return layers[l]; }
     __device__ __forceinline__ int num_layers(const Lane &) const { return P.nl; }
     __device__ __forceinline__ void batch_add(const Lane &L, int slot, unsigned long long v) const {

@@ -262,6 +262,21 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool step_move(Lane &L
     }
     ++L.steps;
     float s;
+#if TMC_BRANCHLESS_STEP
+    {
+        // both candidates, then a select: a fresh free path (which consumes the next word) or the
+        // rest of the one a boundary cut short (which consumes none); the word is read either way
+        // (the ring always holds it) and passed over only when used
+        const bool fresh = L.sleft == 0.0f;
+        const float s_fresh = step_length<FAST>(h, unit_open(C.peek(L)));
+        float s_rest;
+        if constexpr (Math<FAST>::div) s_rest = fmul(L.sleft, h.inv_mut);
+        else s_rest = L.sleft / h.mut;
+        s = fresh ? s_fresh : s_rest;
+        L.rp += fresh ? 1u : 0u;
+        L.sleft = 0.0f;
+    }
+#else
     if (L.sleft == 0.0f) {
         s = step_length<FAST>(h, unit_open(C.draw(L)));
     } else {
@@ -269,6 +284,7 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool step_move(Lane &L
         else s = L.sleft / h.mut;
         L.sleft = 0.0f;
     }
+#endif
     bool hit = false;
     if (L.uz != 0.0f) {
         const float db = m_div<FAST>(fsub(L.uz > 0.0f ? h.z1 : h.z0, L.z), L.uz);
@@ -405,6 +421,8 @@ struct Ring {
     }
     // pass over the next word without reading it
     __device__ __forceinline__ void skip(Lane &L) const { ++L.rp; }
+    // read the next word without passing over it
+    __device__ __forceinline__ uint32_t peek(const Lane &L) const { return base[(L.rp & (kRingWords - 1u)) * slot_stride()]; }
     // each warp's ring is its own region: slot k of its 32 lanes at k * 32 words (a constant stride:
     // the slot addresses take shifts instead of multiplications)
     __device__ __forceinline__ static constexpr int slot_stride() { return 32; }
