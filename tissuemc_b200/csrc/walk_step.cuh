@@ -262,11 +262,12 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool step_move(Lane &L
     }
     ++L.steps;
     float s;
-#if TMC_BRANCHLESS_STEP
     {
         // both candidates, then a select: a fresh free path (which consumes the next word) or the
-        // rest of the one a boundary cut short (which consumes none); the word is read either way
-        // (the ring always holds it) and passed over only when used
+        // rest of the one a boundary cut short (which consumes none). The word is read either way
+        // (the ring always holds it) and passed over only when used. Half of a warp's steps hold a
+        // lane that has just left a boundary, so a branch here diverged; the select measured 5.4 %
+        // faster on skin5.
         const bool fresh = L.sleft == 0.0f;
         const float s_fresh = step_length<FAST>(h, unit_open(C.peek(L)));
         float s_rest;
@@ -276,15 +277,6 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool step_move(Lane &L
         L.rp += fresh ? 1u : 0u;
         L.sleft = 0.0f;
     }
-#else
-    if (L.sleft == 0.0f) {
-        s = step_length<FAST>(h, unit_open(C.draw(L)));
-    } else {
-        if constexpr (Math<FAST>::div) s = fmul(L.sleft, h.inv_mut);
-        else s = L.sleft / h.mut;
-        L.sleft = 0.0f;
-    }
-#endif
     bool hit = false;
     if (L.uz != 0.0f) {
         const float db = m_div<FAST>(fsub(L.uz > 0.0f ? h.z1 : h.z0, L.z), L.uz);
