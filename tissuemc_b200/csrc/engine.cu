@@ -61,6 +61,36 @@ struct DeviceCtx {
 DeviceCtx g_ctx[kMaxDevices];
 std::mutex g_mu;
 
+// The walk kernel for a launch: fast or exact math, with or without a shared core tile of A(r,z).
+const void *walk_kernel_for(bool fast, bool core) {
+    if (fast) return core ? reinterpret_cast<const void *>(walk_kernel<1, true>) : reinterpret_cast<const void *>(walk_kernel<1, false>);
+    return core ? reinterpret_cast<const void *>(walk_kernel<0, true>) : reinterpret_cast<const void *>(walk_kernel<0, false>);
+}
+
+// Every instantiation may use the device's whole opt-in shared memory per block.
+cudaError_t allow_walk_smem(const cudaDeviceProp &prop) {
+    for (int f = 0; f < 2; ++f)
+        for (int c = 0; c < 2; ++c) {
+            const cudaError_t e = cudaFuncSetAttribute(walk_kernel_for(f != 0, c != 0),
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       static_cast<int>(prop.sharedMemPerBlockOptin));
+            if (e != cudaSuccess) return e;
+        }
+    return cudaSuccess;
+}
+
+// Blocks per SM the registers of the walk kernel (with a core tile: the larger of the two) allow.
+int walk_blocks_per_sm(bool fast, int threads) {
+    int bps = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, walk_kernel_for(fast, true), threads, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return bps;
+}
+
+
 void set_status(tmc_status *st, int code, const std::string &msg) {
     if (!st) return;
     st->code = code;
@@ -83,10 +113,7 @@ DeviceCtx &device_ctx(int dev) {
         TMC_CUDA(cudaEventCreate(&c.ev0));
         TMC_CUDA(cudaEventCreate(&c.ev1));
         TMC_CUDA(cudaMalloc(&c.d_counter, 64));
-        TMC_CUDA(cudaFuncSetAttribute(walk_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      c.prop.sharedMemPerBlockOptin));
-        TMC_CUDA(cudaFuncSetAttribute(walk_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      c.prop.sharedMemPerBlockOptin));
+        TMC_CUDA(allow_walk_smem(c.prop));
         c.ready = true;
     }
     return c;
@@ -289,12 +316,8 @@ void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
                  cudaEvent_t e1, uint64_t first = 0, uint64_t count = 0) {
     const RunShape sh = shape_of(spec, opt);
     const size_t words = tally_offsets(sh).total;
-    int regs_bps = 0;
     const int threads = opt.threads_per_block > 0 ? opt.threads_per_block : 256;
-    if (opt.fast_math)
-        TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&regs_bps, walk_kernel<1>, threads, 0));
-    else
-        TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&regs_bps, walk_kernel<0>, threads, 0));
+    const int regs_bps = walk_blocks_per_sm(opt.fast_math != 0, threads);
     const Plan pl = make_plan(spec, opt, limits_of(c.prop), regs_bps);
     WalkParams P = make_params(spec, opt, pl, d_tally, reinterpret_cast<unsigned int *>(counter));
     if (count) {
@@ -310,11 +333,9 @@ void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
     if (e0) TMC_CUDA(cudaEventRecord(e0, stream));
     TMC_CUDA(cudaMemsetAsync(d_tally, 0, words * 8, stream));
     TMC_CUDA(cudaMemsetAsync(counter, 0, 8, stream));
-    if (opt.fast_math)
-        walk_kernel<1><<<grid, pl.threads, smem, stream>>>(P);
-    else
-        walk_kernel<0><<<grid, pl.threads, smem, stream>>>(P);
-    TMC_CUDA(cudaGetLastError());
+    void *args[] = {&P};
+    TMC_CUDA(cudaLaunchKernel(walk_kernel_for(opt.fast_math != 0, pl.tr_a > 0 && pl.tz_a > 0), dim3(grid),
+                              dim3(pl.threads), args, smem, stream));
     if (e1) TMC_CUDA(cudaEventRecord(e1, stream));
 }
 
@@ -390,10 +411,7 @@ StaticDevice &static_device(int dev) {
         void *addr = nullptr;
         TMC_CUDA(cudaGetSymbolAddress(&addr, g_static_scratch));
         d.scratch = static_cast<unsigned long long *>(addr);
-        TMC_CUDA(cudaFuncSetAttribute(walk_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      d.prop.sharedMemPerBlockOptin));
-        TMC_CUDA(cudaFuncSetAttribute(walk_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      d.prop.sharedMemPerBlockOptin));
+        TMC_CUDA(allow_walk_smem(d.prop));
         d.ready = true;
     }
     return d;
@@ -540,12 +558,8 @@ int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_re
         StaticDevice &d = static_device(opt->device);
         unsigned long long *counter = d.scratch;
         unsigned long long *tally = d.scratch + kStaticHeadWords;
-        int regs_bps = 0;
         const int threads = opt->threads_per_block > 0 ? opt->threads_per_block : 256;
-        if (opt->fast_math)
-            TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&regs_bps, walk_kernel<1>, threads, 0));
-        else
-            TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&regs_bps, walk_kernel<0>, threads, 0));
+        const int regs_bps = walk_blocks_per_sm(opt->fast_math != 0, threads);
         const Plan pl = make_plan(*spec, *opt, limits_of(d.prop), regs_bps);
         WalkParams P = make_params(*spec, *opt, pl, tally, reinterpret_cast<unsigned int *>(counter));
         const size_t smem = plan_smem_bytes(P);
@@ -556,11 +570,9 @@ int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_re
         // the array keeps the previous call's contents: the counter and the tallies start at zero
         TMC_CUDA(cudaMemsetAsync(d.scratch, 0, (kStaticHeadWords + words) * 8, 0));
         const auto k0 = std::chrono::steady_clock::now();
-        if (opt->fast_math)
-            walk_kernel<1><<<grid, pl.threads, smem, 0>>>(P);
-        else
-            walk_kernel<0><<<grid, pl.threads, smem, 0>>>(P);
-        TMC_CUDA(cudaGetLastError());
+        void *args[] = {&P};
+        TMC_CUDA(cudaLaunchKernel(walk_kernel_for(opt->fast_math != 0, pl.tr_a > 0 && pl.tz_a > 0), dim3(grid),
+                                  dim3(pl.threads), args, smem, 0));
         TMC_CUDA(cudaStreamSynchronize(0));
         const auto k1 = std::chrono::steady_clock::now();
         TMC_CUDA(cudaMemcpy(res->raw, tally, words * 8, cudaMemcpyDeviceToHost));
@@ -603,13 +615,7 @@ int tmc_b200_autotune(const tmc_run_spec *spec, tmc_options *opt, uint64_t sampl
         base.batches = static_cast<int32_t>(std::min<uint64_t>(static_cast<uint64_t>(base.batches), base.photons));
         ensure_tally(c, tally_offsets(shape_of(*spec, base)).total);
         auto regs_blocks = [&](const tmc_options &o) {
-            int bps = 0;
-            const int threads = o.threads_per_block > 0 ? o.threads_per_block : 256;
-            if (o.fast_math)
-                TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, walk_kernel<1>, threads, 0));
-            else
-                TMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, walk_kernel<0>, threads, 0));
-            return bps;
+            return walk_blocks_per_sm(o.fast_math != 0, o.threads_per_block > 0 ? o.threads_per_block : 256);
         };
         auto time_of = [&](const tmc_options &o) -> double {
             const Plan pl = make_plan(*spec, o, limits_of(c.prop), regs_blocks(o));

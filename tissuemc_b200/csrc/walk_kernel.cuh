@@ -49,7 +49,9 @@ __host__ __device__ inline SmemLayout smem_layout(const WalkParams &P) {
 
 // Where one run's walk keeps its layer table and tallies: a shared-memory layer table, per-batch
 // totals and profile tiles privatised in shared memory (the rest in global memory).
-template <int FAST> struct PlainCtx {
+// CORE: the plan has a shared core tile of A(r,z) (tr_a, tz_a > 0); without one the kernel is a
+// separate instantiation that does not test for it.
+template <int FAST, bool CORE> struct PlainCtx {
     const WalkParams &P;
     Ring ring;  // refilled with the launch's precomputed Philox key schedule (P.round_keys)
     uint32_t step_cap;
@@ -77,11 +79,11 @@ template <int FAST> struct PlainCtx {
         unsigned long long *p = &P.g_arz[static_cast<size_t>(ir) * P.nz + iz];
         if (cross && ir == P.nr - 1) p = &s_lastr[iz];
         if (cross && iz == P.nz - 1) p = &s_lastz[ir];
-        if (ir < P.tr_a && iz < P.tz_a) p = &s_core[ir * P.tz_a + iz];
+        if (CORE && ir < P.tr_a && iz < P.tz_a) p = &s_core[ir * P.tz_a + iz];
         atomicAdd(p, v);
         return;
 #endif
-        if (ir < P.tr_a && iz < P.tz_a) {
+        if (CORE && ir < P.tr_a && iz < P.tz_a) {
             atomicAdd(&s_core[ir * P.tz_a + iz], v);
         } else if (cross && iz == P.nz - 1) {
             atomicAdd(&s_lastz[ir], v);
@@ -129,7 +131,7 @@ template <int FAST> struct PlainCtx {
 #define TMC_WALK_BOUNDS __launch_bounds__(256)
 #endif
 
-template <int FAST>
+template <int FAST, bool CORE>
 __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P) {
     extern __shared__ __align__(16) unsigned long long smem[];
     const SmemLayout S = smem_layout(P);
@@ -140,7 +142,7 @@ __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P
         for (int i = threadIdx.x; i < P.nl * static_cast<int>(sizeof(LayerC) / 4); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
-    PlainCtx<FAST> C{P,
+    PlainCtx<FAST, CORE> C{P,
                      Ring{reinterpret_cast<uint32_t *>(smem + S.ring) + ring_lane_offset()},
                      P.step_cap,
                      reinterpret_cast<const LayerC *>(smem + S.layers),
@@ -204,7 +206,7 @@ __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P
             if (v) atomicAdd(&P.g_batch[i], v);
         }
     }
-    for (int i = threadIdx.x; i < P.tr_a * P.tz_a; i += blockDim.x) {
+    for (int i = threadIdx.x; i < (CORE ? P.tr_a * P.tz_a : 0); i += blockDim.x) {
         const unsigned long long v = C.s_core[i];
         if (v) atomicAdd(&P.g_arz[static_cast<size_t>(i / P.tz_a) * P.nz + (i % P.tz_a)], v);
     }
