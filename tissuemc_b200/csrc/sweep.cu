@@ -19,6 +19,13 @@
 #include "engine_internal.hpp"
 #include "sweep_kernel.cuh"
 
+#ifndef TMC_SWEEP_STRIDE_PAD
+#define TMC_SWEEP_STRIDE_PAD 0
+#endif
+#ifndef TMC_SWEEP_TALLY_OFFSET
+#define TMC_SWEEP_TALLY_OFFSET 0
+#endif
+
 namespace tmc {
 // shared with the single-run loop in engine.cu
 void sweep_block_to_layout(const uint64_t *src, int lmax, int nl, const tmc_sweep_options &o, uint64_t *dst);
@@ -160,6 +167,7 @@ struct SweepGraph {
     unsigned char *d_blob = nullptr, *h_blob = nullptr;
     size_t blob_bytes = 0, off_cfg = 0, off_prefix = 0, off_layers = 0;
     unsigned long long *d_tally = nullptr;
+    void *d_tally_alloc = nullptr;  // the allocation d_tally lies in
     unsigned int *d_counter = nullptr;
     double *d_summary = nullptr, *h_summary = nullptr;
     std::vector<int> order;  // table slot -> the caller's configuration (longest photons first)
@@ -171,7 +179,7 @@ struct SweepGraph {
         if (e1) cudaEventDestroy(e1);
         if (stream) cudaStreamDestroy(stream);
         cudaFree(d_blob);
-        cudaFree(d_tally);
+        cudaFree(d_tally_alloc);
         cudaFree(d_counter);
         cudaFree(d_summary);
         cudaFreeHost(h_blob);
@@ -204,7 +212,7 @@ std::unique_ptr<SweepGraph> build_graph(int cap, int lmax, const tmc_sweep_optio
     g->cap_cfg = cap;
     g->lmax = lmax;
     g->stride = static_cast<size_t>(o.batches) * (4 + lmax) + static_cast<size_t>(o.nr) * o.nz +
-                2 * static_cast<size_t>(o.nr) * o.na;
+                2 * static_cast<size_t>(o.nr) * o.na + TMC_SWEEP_STRIDE_PAD;
     g->threads = o.threads_per_block > 0 ? o.threads_per_block : 256;
     // per lane: the random-word ring (kRingWords words) and the Philox key schedule (5 x 16 bytes);
     // per warp: the optional tile of A(r,z)
@@ -229,7 +237,9 @@ std::unique_ptr<SweepGraph> build_graph(int cap, int lmax, const tmc_sweep_optio
     g->blob_bytes = g->off_layers + align_up(sizeof(LayerC) * static_cast<size_t>(cap) * lmax);
     SW_CUDA(cudaMalloc(&g->d_blob, g->blob_bytes));
     SW_CUDA(cudaMallocHost(&g->h_blob, g->blob_bytes));
-    SW_CUDA(cudaMalloc(&g->d_tally, g->stride * cap * 8));
+    SW_CUDA(cudaMalloc(&g->d_tally_alloc, g->stride * cap * 8 + TMC_SWEEP_TALLY_OFFSET));
+    g->d_tally = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(g->d_tally_alloc) +
+                                                        TMC_SWEEP_TALLY_OFFSET);
     SW_CUDA(cudaMalloc(&g->d_counter, 256));
     const size_t sum_words = static_cast<size_t>(cap) * (o.nr + 3);
     SW_CUDA(cudaMalloc(&g->d_summary, sum_words * 8));
@@ -512,7 +522,7 @@ int tmc_b200_sweep_run(const tmc_sweep_config *cfgs, int32_t n, const tmc_sweep_
             for (int slot = 0; slot < n; ++slot) {
                 const uint64_t *src = all.data() + static_cast<size_t>(slot) * g.stride;
                 uint64_t *dst = raw + static_cast<size_t>(g.order[slot]) * sh.stride;
-                if (g.lmax == sh.lmax) std::memcpy(dst, src, g.stride * 8);
+                if (g.lmax == sh.lmax) std::memcpy(dst, src, sh.stride * 8);  // any padding stays behind
                 else sweep_to_run_layout(src, g.lmax, sh.lmax, *opt, dst);
             }
         }
