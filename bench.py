@@ -84,6 +84,9 @@ def _args():
     ap.add_argument("--no-loop", action="store_true", help="sweep: skip the single-run loop baseline (diagnostic)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="walk: use the planner's default launch and tile plan instead of autotuning it")
+    ap.add_argument("--tile-tz", type=int, default=None,
+                    help="walk: the depth of the shared core tile (-1: none), instead of autotuning the plan "
+                         "(for profiling one plan)")
     ap.add_argument("--no-extras", action="store_true",
                     help="default line only: skip the sweep, serve and reference-GPU sub-measurements")
     ap.add_argument("--no-profiles", action="store_true",
@@ -544,9 +547,9 @@ def main() -> None:
     spec.photons = photons * world
     first, count = tmc.shard_range(spec.photons, rank, world)
     opt = tmc.options(batches=a.batches, seed=1, device=local, rung=6 if a.no_profiles else 0,
-                      profiles=not a.no_profiles)
+                      profiles=not a.no_profiles, tile_tz=a.tile_tz or 0)
     tuning = None
-    if not a.no_autotune:
+    if not a.no_autotune and a.tile_tz is None:
         # the launch and tally-tile plan, picked by timing candidates on a 2e7-photon sample of
         # this run (tmc_b200_autotune); the results do not depend on it
         opt, plan, t_default, t_best = tmc.autotune(spec, opt, sample_photons=min(spec.photons, 20_000_000))

@@ -396,8 +396,8 @@ def test_autotuned_plan_gives_the_same_tallies(skin):
     b = tmc.run(skin, tuned)
     assert np.array_equal(a.raw, b.raw)
     # the tile options on their own, each away from the planner's choice
-    for kw in ({"tile_cross": -1}, {"tile_ra_rows": -1}, {"tile_tz": 399}, {"blocks_per_sm": 2},
-               {"threads_per_block": 128}):
+    for kw in ({"tile_cross": -1}, {"tile_ra_rows": -1}, {"tile_tz": 399}, {"tile_tz": -1},
+               {"tile_tz": -1, "tile_cross": -1}, {"blocks_per_sm": 2}, {"threads_per_block": 128}):
         o = tmc.options(photons=300_000, batches=20, seed=4, **kw)
         assert np.array_equal(tmc.run(skin, o).raw, tmc.run(skin, photons=300_000, batches=20, seed=4).raw), kw
 
