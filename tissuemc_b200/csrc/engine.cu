@@ -119,6 +119,17 @@ DeviceCtx &device_ctx(int dev) {
     return c;
 }
 
+// Blocks of `kern` that can be resident on the whole device at once with this dynamic shared memory
+// (at least one wave's worth of one block per SM, so a launch always makes progress).
+uint64_t resident_blocks(const void *kern, const cudaDeviceProp &prop, int threads, size_t smem) {
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        occ = 1;
+    }
+    return static_cast<uint64_t>(prop.multiProcessorCount) * static_cast<uint64_t>(std::max(1, occ));
+}
+
 DeviceLimits limits_of(const cudaDeviceProp &p) {
     return DeviceLimits{p.multiProcessorCount, p.sharedMemPerMultiprocessor, p.sharedMemPerBlockOptin,
                         p.reservedSharedMemPerBlock};
@@ -327,15 +338,17 @@ void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
     const size_t smem = plan_smem_bytes(P);
     if (smem > c.prop.sharedMemPerBlockOptin)
         throw Fail(TMC_BAD_CONFIG, "the tally plan does not fit in shared memory");
-    // never more lanes than photons: whole blocks only
+    // never more lanes than photons (whole blocks only), and never more blocks than can be resident
+    // at once with this plan's shared memory: the kernel is persistent, a second wave would idle
+    const void *kern = walk_kernel_for(opt.fast_math != 0, pl.tr_a > 0 && pl.tz_a > 0);
     const uint64_t max_blocks = (P.photons + pl.threads - 1) / pl.threads;
-    const int grid = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(pl.grid), max_blocks));
+    const int grid = static_cast<int>(
+        std::min<uint64_t>({static_cast<uint64_t>(pl.grid), max_blocks, resident_blocks(kern, c.prop, pl.threads, smem)}));
     if (e0) TMC_CUDA(cudaEventRecord(e0, stream));
     TMC_CUDA(cudaMemsetAsync(d_tally, 0, words * 8, stream));
     TMC_CUDA(cudaMemsetAsync(counter, 0, 8, stream));
     void *args[] = {&P};
-    TMC_CUDA(cudaLaunchKernel(walk_kernel_for(opt.fast_math != 0, pl.tr_a > 0 && pl.tz_a > 0), dim3(grid),
-                              dim3(pl.threads), args, smem, stream));
+    TMC_CUDA(cudaLaunchKernel(kern, dim3(grid), dim3(pl.threads), args, smem, stream));
     if (e1) TMC_CUDA(cudaEventRecord(e1, stream));
 }
 
@@ -565,14 +578,15 @@ int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_re
         const size_t smem = plan_smem_bytes(P);
         if (smem > d.prop.sharedMemPerBlockOptin)
             throw Fail(TMC_BAD_CONFIG, "the tally plan does not fit in shared memory");
+        const void *kern = walk_kernel_for(opt->fast_math != 0, pl.tr_a > 0 && pl.tz_a > 0);
         const uint64_t max_blocks = (sh.photons + pl.threads - 1) / pl.threads;
-        const int grid = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(pl.grid), max_blocks));
+        const int grid = static_cast<int>(std::min<uint64_t>(
+            {static_cast<uint64_t>(pl.grid), max_blocks, resident_blocks(kern, d.prop, pl.threads, smem)}));
         // the array keeps the previous call's contents: the counter and the tallies start at zero
         TMC_CUDA(cudaMemsetAsync(d.scratch, 0, (kStaticHeadWords + words) * 8, 0));
         const auto k0 = std::chrono::steady_clock::now();
         void *args[] = {&P};
-        TMC_CUDA(cudaLaunchKernel(walk_kernel_for(opt->fast_math != 0, pl.tr_a > 0 && pl.tz_a > 0), dim3(grid),
-                                  dim3(pl.threads), args, smem, 0));
+        TMC_CUDA(cudaLaunchKernel(kern, dim3(grid), dim3(pl.threads), args, smem, 0));
         TMC_CUDA(cudaStreamSynchronize(0));
         const auto k1 = std::chrono::steady_clock::now();
         TMC_CUDA(cudaMemcpy(res->raw, tally, words * 8, cudaMemcpyDeviceToHost));
