@@ -79,10 +79,11 @@ cudaError_t allow_walk_smem(const cudaDeviceProp &prop) {
     return cudaSuccess;
 }
 
-// Blocks per SM the registers of the walk kernel (with a core tile: the larger of the two) allow.
-int walk_blocks_per_sm(bool fast, int threads) {
+// Blocks per SM the registers of the walk kernel allow: the instantiation without a core tile when
+// the options rule the core tile out (tile_tz = -1), else the one with it (the larger of the two).
+int walk_blocks_per_sm(bool fast, int threads, bool core) {
     int bps = 0;
-    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, walk_kernel_for(fast, true), threads, 0);
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, walk_kernel_for(fast, core), threads, 0);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -177,7 +178,11 @@ Plan make_plan(const tmc_run_spec &spec, const tmc_options &opt, const DeviceLim
     budget = std::max(budget, layer_bytes + ring_bytes + 16);
     size_t rem = budget - layer_bytes - ring_bytes - 16;
     const size_t batch_bytes = static_cast<size_t>(sh.nb) * (4 + sh.nl) * 8;
-    p.batch_smem = batch_bytes <= rem / 4 ? 1 : 0;
+    // The batch totals come first (up to half of what is left): every photon publishes into its
+    // batch's words, and photon ids are claimed in order, so the lanes of the whole device are in one
+    // or two batches at a time; in global memory those same-address atomics serialise in L2 (skin5,
+    // 192 threads x 6 blocks per SM: 921 ms with the totals in global memory, 619 ms in shared).
+    p.batch_smem = batch_bytes <= rem / 2 ? 1 : 0;
     if (p.batch_smem) rem -= batch_bytes;
     const size_t nr = sh.nr, nz = sh.nz, na = sh.na;
     if (opt.profiles) {
@@ -328,7 +333,7 @@ void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
     const RunShape sh = shape_of(spec, opt);
     const size_t words = tally_offsets(sh).total;
     const int threads = opt.threads_per_block > 0 ? opt.threads_per_block : 256;
-    const int regs_bps = walk_blocks_per_sm(opt.fast_math != 0, threads);
+    const int regs_bps = walk_blocks_per_sm(opt.fast_math != 0, threads, opt.tile_tz != -1);
     const Plan pl = make_plan(spec, opt, limits_of(c.prop), regs_bps);
     WalkParams P = make_params(spec, opt, pl, d_tally, reinterpret_cast<unsigned int *>(counter));
     if (count) {
@@ -572,7 +577,7 @@ int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_re
         unsigned long long *counter = d.scratch;
         unsigned long long *tally = d.scratch + kStaticHeadWords;
         const int threads = opt->threads_per_block > 0 ? opt->threads_per_block : 256;
-        const int regs_bps = walk_blocks_per_sm(opt->fast_math != 0, threads);
+        const int regs_bps = walk_blocks_per_sm(opt->fast_math != 0, threads, opt->tile_tz != -1);
         const Plan pl = make_plan(*spec, *opt, limits_of(d.prop), regs_bps);
         WalkParams P = make_params(*spec, *opt, pl, tally, reinterpret_cast<unsigned int *>(counter));
         const size_t smem = plan_smem_bytes(P);
@@ -629,7 +634,8 @@ int tmc_b200_autotune(const tmc_run_spec *spec, tmc_options *opt, uint64_t sampl
         base.batches = static_cast<int32_t>(std::min<uint64_t>(static_cast<uint64_t>(base.batches), base.photons));
         ensure_tally(c, tally_offsets(shape_of(*spec, base)).total);
         auto regs_blocks = [&](const tmc_options &o) {
-            return walk_blocks_per_sm(o.fast_math != 0, o.threads_per_block > 0 ? o.threads_per_block : 256);
+            return walk_blocks_per_sm(o.fast_math != 0, o.threads_per_block > 0 ? o.threads_per_block : 256,
+                                      o.tile_tz != -1);
         };
         auto time_of = [&](const tmc_options &o) -> double {
             const Plan pl = make_plan(*spec, o, limits_of(c.prop), regs_blocks(o));
@@ -687,6 +693,16 @@ int tmc_b200_autotune(const tmc_run_spec *spec, tmc_options *opt, uint64_t sampl
             if (rows == 0) continue;
             tmc_options o = best;
             o.tile_ra_rows = rows;
+            try_opt(o);
+        }
+        // block sizes again, with the chosen tiles: without a core tile the kernel holds fewer
+        // registers, and blocks of 6 or 7 warps fit more warps per SM than 8 (skin5: 36 warps of
+        // 192-thread blocks, 0.75 % faster than 32 of 256 at full size)
+        for (int threads : {192, 224, 128}) {
+            if (threads == (best.threads_per_block > 0 ? best.threads_per_block : 256)) continue;
+            tmc_options o = best;
+            o.threads_per_block = threads;
+            o.blocks_per_sm = 0;
             try_opt(o);
         }
         opt->threads_per_block = best.threads_per_block;

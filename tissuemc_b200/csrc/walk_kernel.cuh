@@ -7,8 +7,10 @@
 
 namespace tmc {
 
-// 1 (default): route a deposit with selects and one generic-address atomic, no divergent paths
-// (measured 2.1 % faster on skin5); 0: branch to the shared or the global atomic
+// 1 (default): route a deposit with selects and one generic-address atomic, no divergent paths; 0:
+// branch to the shared or the global atomic. On skin5 the branching form measured 2.1 % slower with
+// a shared core tile and 30 % slower (811 against 624 ms for 1e8 photons) without one, where the
+// lanes of a warp split between the shared last row and column and global memory at most steps.
 #ifndef TMC_DEPOSIT_GENERIC
 #define TMC_DEPOSIT_GENERIC 1
 #endif
