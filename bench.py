@@ -87,6 +87,8 @@ def _args():
     ap.add_argument("--tile-tz", type=int, default=None,
                     help="walk: the depth of the shared core tile (-1: none), instead of autotuning the plan "
                          "(for profiling one plan)")
+    ap.add_argument("--threads", type=int, default=0,
+                    help="walk: threads per block of the plan given by --tile-tz (0: the planner's 256)")
     ap.add_argument("--no-extras", action="store_true",
                     help="default line only: skip the sweep, serve and reference-GPU sub-measurements")
     ap.add_argument("--no-profiles", action="store_true",
@@ -548,6 +550,8 @@ def main() -> None:
     first, count = tmc.shard_range(spec.photons, rank, world)
     opt = tmc.options(batches=a.batches, seed=1, device=local, rung=6 if a.no_profiles else 0,
                       profiles=not a.no_profiles, tile_tz=a.tile_tz or 0)
+    if a.tile_tz is not None:
+        opt.threads_per_block = a.threads
     tuning = None
     if not a.no_autotune and a.tile_tz is None:
         # the launch and tally-tile plan, picked by timing candidates on a 2e7-photon sample of
