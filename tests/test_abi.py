@@ -169,6 +169,22 @@ def test_plan_follows_the_tile_options():
             tmc.plan(skin, tmc.options(batches=100, **bad))
 
 
+def test_plan_keeps_the_batch_totals_and_the_cross_before_rows():
+    """The batch totals and the cross (the clamped last row and column of A(r,z)) are the words every
+    running photon shares; the planner places them before the rows of R_d(r,a) and T_t(r,a), so a
+    smaller budget per block (smaller blocks, more of them) or a request for many rows costs rows,
+    not the shared words."""
+    skin = tmc.workload("skin5")
+    for threads, bps in ((256, 4), (224, 5), (192, 6), (128, 9)):
+        o = tmc.options(batches=100, tile_tz=-1)
+        o.threads_per_block = threads
+        p = tmc.plan(skin, o, regs_blocks_per_sm=bps)
+        assert p.batch_smem == 1 and p.cross == 1, (threads, bps)
+        assert p.smem_bytes <= min(232448, 233472 // bps - 1024)
+    p = tmc.plan(skin, tmc.options(batches=100, tile_tz=-1, tile_ra_rows=500))
+    assert p.cross == 1 and 17 < p.tr_rd < 500
+
+
 def test_plan_smem_per_block_never_exceeds_the_device():
     rng = np.random.default_rng(0)
     for _ in range(200):
