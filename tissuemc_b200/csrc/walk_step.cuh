@@ -39,6 +39,7 @@ constexpr uint32_t kRingWords = TMC_RING_WORDS;
 #define TMC_HOT_SMEM 0
 #endif
 constexpr bool kHotInSmem = TMC_HOT_SMEM != 0;
+
 static_assert(kRingWords == 8 || kRingWords == 16, "ring of 8 or 16 words");
 
 constexpr float kCosZero = 1.0f - 1e-6f;  // physics.hpp:35 (float widening of MCML COSZERO)
@@ -355,27 +356,31 @@ template <int FAST, class Ctx> __device__ __forceinline__ void step_interaction(
 // an ended packet (unless the kernel does: Ctx::kPublishAtRelaunch). Returns true when the packet
 // has ended.
 template <int FAST, class Ctx> __device__ __forceinline__ bool step_tail(Lane &L, Ctx &C, int exit_kind, bool died) {
-    if (exit_kind) {
-        // ---- score the exit (check, totals, R_d(r,a) or T_t(r,a))
-        const float n2 = norm2(L.uxy, L.uz);
-        if (!(L.w == L.w) || !(fabsf(fsub(n2, 1.0f)) <= 1e-5f)) ++L.anomalies;
-        const unsigned long long v = to_fixed(L.w);
-        C.batch_add(L, exit_kind - 1, v);
-        C.exit(L, exit_kind, v);
-    } else if (L.w < kWeightMin) {
-        // ---- roulette (physics.hpp:250-259)
-        if (L.w == 0.0f) {
-            died = true;
-        } else if (unit_open(C.draw(L)) < kChance) {
-            if constexpr (Math<FAST>::div) L.w = fmul(L.w, 10.0f);
-            else L.w /= kChance;
-        } else {
+    // one test on the common path for the three rare ends of a step: an exit, a weight below the
+    // roulette threshold, the step cap (measured 0.4 % faster on skin5 than three tests)
+    if (exit_kind != 0 || L.w < kWeightMin || L.steps >= C.step_cap) {
+        if (exit_kind) {
+            // ---- score the exit (check, totals, R_d(r,a) or T_t(r,a))
+            const float n2 = norm2(L.uxy, L.uz);
+            if (!(L.w == L.w) || !(fabsf(fsub(n2, 1.0f)) <= 1e-5f)) ++L.anomalies;
+            const unsigned long long v = to_fixed(L.w);
+            C.batch_add(L, exit_kind - 1, v);
+            C.exit(L, exit_kind, v);
+        } else if (L.w < kWeightMin) {
+            // ---- roulette (physics.hpp:250-259)
+            if (L.w == 0.0f) {
+                died = true;
+            } else if (unit_open(C.draw(L)) < kChance) {
+                if constexpr (Math<FAST>::div) L.w = fmul(L.w, 10.0f);
+                else L.w /= kChance;
+            } else {
+                died = true;
+            }
+        }
+        if (!died && L.steps >= C.step_cap) {  // a packet that never ends is an anomaly, not a hang
+            ++L.anomalies;
             died = true;
         }
-    }
-    if (!died && L.steps >= C.step_cap) {  // a packet that never ends is an anomaly, not a hang
-        ++L.anomalies;
-        died = true;
     }
     if constexpr (!Ctx::kPublishAtRelaunch) {
         if (died) finish_photon(L, C);
