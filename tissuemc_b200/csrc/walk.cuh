@@ -9,9 +9,10 @@
 //  * a lane is one thread of a persistent, warp-synchronous loop; a lane whose photon ends claims
 //    the next id from a per-warp pool, which the warp refills from a global counter in chunks;
 //  * all photon state and the hot constants of the current layer live in registers; the random
-//    words wait in an 8-word ring per lane in shared memory (walk_step.cuh, Ring), refilled with
-//    one Philox block whenever fewer than the four a step may draw are left; the layer table lives
-//    in shared memory and is read only when a packet changes layer or meets a boundary;
+//    words wait in a 16-word ring per lane in shared memory (walk_step.cuh, Ring), refilled with
+//    one Philox block by every lane of the warp with room for it whenever any lane has fewer than
+//    the four a step may draw; the layer table lives in shared memory and is read only when a
+//    packet changes layer or meets a boundary;
 //  * every tally is an unsigned 64-bit fixed-point integer (weight * 2^32, rounded), so sums are
 //    exact and a run's output does not depend on scheduling; per-photon values (events, absorbed
 //    weight in the current layer, the exit weight) accumulate in registers and are published once
