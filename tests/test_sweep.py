@@ -162,6 +162,23 @@ def test_summaries_follow_from_the_tallies():
 
 
 @pytest.mark.gpu
+def test_sweep_of_totals_only_keeps_the_batch_totals():
+    """Without profile tallies (profiles = 0, a kernel of its own) every configuration's batch totals
+    (R_d, T_t, events, anomalies, absorbed weight per layer) are the same bits as with them, and the
+    profile words stay zero."""
+    cfgs = _scaled(tmc.sweep_sample(13, 64), 5000)
+    on = tmc.sweep_run(cfgs, tmc.sweep_options(), raw=True)
+    off = tmc.sweep_run(cfgs, tmc.sweep_options(profiles=0), raw=True)
+    opt = tmc.sweep_options()
+    nb = opt.batches
+    lmax = (on.raw.shape[1] - opt.nr * opt.nz - 2 * opt.nr * opt.na) // nb - 4
+    head = nb * (4 + lmax)
+    assert np.array_equal(on.raw[:, :head], off.raw[:, :head])
+    assert not off.raw[:, head:].any() and on.raw[:, head:].any()
+    assert np.array_equal(on.summary[:, opt.nr:], off.summary[:, opt.nr:])
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("tile", [(8, 8), (16, 16), (16, 32), (64, 4)])
 def test_per_warp_tile_gives_the_same_tallies(tile):
     """Deposits of the configuration a warp is working on go to the warp's shared tile and are

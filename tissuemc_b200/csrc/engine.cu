@@ -62,7 +62,9 @@ DeviceCtx g_ctx[kMaxDevices];
 std::mutex g_mu;
 
 // The walk kernel for a launch: fast or exact math, with or without a shared core tile of A(r,z).
-const void *walk_kernel_for(bool fast, bool core) {
+const void *walk_kernel_for(bool fast, bool core, bool profiles = true) {
+    if (!profiles) return fast ? reinterpret_cast<const void *>(walk_kernel_totals<1>)
+                               : reinterpret_cast<const void *>(walk_kernel_totals<0>);
     if (fast) return core ? reinterpret_cast<const void *>(walk_kernel<1, true>) : reinterpret_cast<const void *>(walk_kernel<1, false>);
     return core ? reinterpret_cast<const void *>(walk_kernel<0, true>) : reinterpret_cast<const void *>(walk_kernel<0, false>);
 }
@@ -70,8 +72,8 @@ const void *walk_kernel_for(bool fast, bool core) {
 // Every instantiation may use the device's whole opt-in shared memory per block.
 cudaError_t allow_walk_smem(const cudaDeviceProp &prop) {
     for (int f = 0; f < 2; ++f)
-        for (int c = 0; c < 2; ++c) {
-            const cudaError_t e = cudaFuncSetAttribute(walk_kernel_for(f != 0, c != 0),
+        for (int k = 0; k < 3; ++k) {
+            const cudaError_t e = cudaFuncSetAttribute(walk_kernel_for(f != 0, k == 1, k != 2),
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        static_cast<int>(prop.sharedMemPerBlockOptin));
             if (e != cudaSuccess) return e;
@@ -349,7 +351,7 @@ void launch_walk(const tmc_run_spec &spec, const tmc_options &opt, DeviceCtx &c,
         throw Fail(TMC_BAD_CONFIG, "the tally plan does not fit in shared memory");
     // never more lanes than photons (whole blocks only), and never more blocks than can be resident
     // at once with this plan's shared memory: the kernel is persistent, a second wave would idle
-    const void *kern = walk_kernel_for(opt.fast_math != 0, pl.tr_a > 0 && pl.tz_a > 0);
+    const void *kern = walk_kernel_for(opt.fast_math != 0, pl.tr_a > 0 && pl.tz_a > 0, P.profiles != 0);
     const uint64_t max_blocks = (P.photons + pl.threads - 1) / pl.threads;
     const int grid = static_cast<int>(
         std::min<uint64_t>({static_cast<uint64_t>(pl.grid), max_blocks, resident_blocks(kern, c.prop, pl.threads, smem)}));
@@ -587,7 +589,7 @@ int tmc_b200_run_static(const tmc_run_spec *spec, const tmc_options *opt, tmc_re
         const size_t smem = plan_smem_bytes(P);
         if (smem > d.prop.sharedMemPerBlockOptin)
             throw Fail(TMC_BAD_CONFIG, "the tally plan does not fit in shared memory");
-        const void *kern = walk_kernel_for(opt->fast_math != 0, pl.tr_a > 0 && pl.tz_a > 0);
+        const void *kern = walk_kernel_for(opt->fast_math != 0, pl.tr_a > 0 && pl.tz_a > 0, P.profiles != 0);
         const uint64_t max_blocks = (sh.photons + pl.threads - 1) / pl.threads;
         const int grid = static_cast<int>(std::min<uint64_t>(
             {static_cast<uint64_t>(pl.grid), max_blocks, resident_blocks(kern, d.prop, pl.threads, smem)}));

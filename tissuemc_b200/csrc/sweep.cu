@@ -221,12 +221,15 @@ std::unique_ptr<SweepGraph> build_graph(int cap, int lmax, const tmc_sweep_optio
               static_cast<size_t>(g->threads / 32) * o.tile_r * o.tile_z * 8;
     cudaDeviceProp prop;
     SW_CUDA(cudaGetDeviceProperties(&prop, o.device));
-    // the kernel for these options: fast or exact math, with or without the per-warp tile
+    // the kernel for these options: fast or exact math, with or without the per-warp tile, or the
+    // kernel of totals only (no profile tallies)
     const bool tile = o.profiles && o.tile_r > 0;
-    const void *kern = o.fast_math ? (tile ? reinterpret_cast<const void *>(sweep_kernel<1, true>)
-                                           : reinterpret_cast<const void *>(sweep_kernel<1, false>))
-                                   : (tile ? reinterpret_cast<const void *>(sweep_kernel<0, true>)
-                                           : reinterpret_cast<const void *>(sweep_kernel<0, false>));
+    const void *kern = !o.profiles ? (o.fast_math ? reinterpret_cast<const void *>(sweep_kernel_totals<1>)
+                                                  : reinterpret_cast<const void *>(sweep_kernel_totals<0>))
+                       : o.fast_math ? (tile ? reinterpret_cast<const void *>(sweep_kernel<1, true>)
+                                             : reinterpret_cast<const void *>(sweep_kernel<1, false>))
+                                     : (tile ? reinterpret_cast<const void *>(sweep_kernel<0, true>)
+                                             : reinterpret_cast<const void *>(sweep_kernel<0, false>));
     SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(g->smem)));
     int bps = 0;
     SW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, g->threads, g->smem));

