@@ -73,6 +73,12 @@ constexpr int kNoCacheKey = 0x7FFFFFFF;  // the run cache is empty (tally word i
 // 0 (default): every deposit goes straight to its word; 1: a per-lane run cache merges consecutive
 // deposits into one A(r,z) bin (measured 5 % slower on the 4096-configuration sweep: its branch
 // costs more than the atomics it saves)
+// Steps a lane takes per pass of the sweep's loop: 1 (two measured no faster, the kernel held to 64
+// registers spilling)
+#ifndef TMC_SWEEP_STEPS_PER_ITER
+#define TMC_SWEEP_STEPS_PER_ITER 1
+#endif
+
 #ifndef TMC_SWEEP_RUN_CACHE
 #define TMC_SWEEP_RUN_CACHE 0
 #endif
@@ -111,7 +117,8 @@ template <int FAST, bool TILE, bool PROF> struct SweepCtx {
         atomicAdd(&P.tally[t + L.batch * bstride + slot], v);
     }
     __device__ __forceinline__ void deposit(int key, unsigned long long v) const {
-        if (key < 0) atomicAdd(&tile[-1 - key], v);
+        // negative keys name the warp's tile, which only the TILE instantiation has
+        if (TILE && key < 0) atomicAdd(&tile[-1 - key], v);
         else atomicAdd(&P.tally[key], v);
     }
     __device__ __forceinline__ void absorb(const Lane &L, unsigned long long v) {
@@ -269,7 +276,13 @@ __device__ __forceinline__ void sweep_body(const SweepParams &P) {
         }
         if (ex_mask == 0xffffffffu) break;  // exhausted lanes hold no photon: the warp is done
         if (!alive) continue;
-        if (walk_step<FAST>(L, C)) alive = false;
+        {
+            bool ended = false;
+#pragma unroll
+            for (int k = 0; k < TMC_SWEEP_STEPS_PER_ITER; ++k)
+                if (!ended) ended = walk_step<FAST>(L, C);
+            if (ended) alive = false;
+        }
     }
     C.flush_cache();
     if constexpr (TILE) C.flush_tile(lane);
