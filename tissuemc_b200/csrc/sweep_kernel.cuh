@@ -73,14 +73,22 @@ constexpr int kNoCacheKey = 0x7FFFFFFF;  // the run cache is empty (tally word i
 // 0 (default): every deposit goes straight to its word; 1: a per-lane run cache merges consecutive
 // deposits into one A(r,z) bin (measured 5 % slower on the 4096-configuration sweep: its branch
 // costs more than the atomics it saves)
-// Steps a lane takes per pass of the sweep's loop: 1 (two measured no faster, the kernel held to 64
-// registers spilling)
-#ifndef TMC_SWEEP_STEPS_PER_ITER
-#define TMC_SWEEP_STEPS_PER_ITER 1
-#endif
-
 #ifndef TMC_SWEEP_RUN_CACHE
 #define TMC_SWEEP_RUN_CACHE 0
+#endif
+
+// Steps a lane takes per pass of the sweep's loop (the relaunch ballot and the live test once per
+// pass). Measured on the 4096-configuration sweep: 1 1.303 s, 2 1.305 s (the kernel, held to 64
+// registers, spills), 3 1.286 s.
+#ifndef TMC_SWEEP_STEPS_PER_ITER
+#define TMC_SWEEP_STEPS_PER_ITER 3
+#endif
+
+// 1: an ended packet's totals are published when its lane relaunches (as in the single-run kernel)
+// instead of in the step; measured 0.9 % slower with one step per pass and 0.5 % faster with three
+// (within the noise, and the kernel spills), so 0
+#ifndef TMC_SWEEP_PUBLISH_AT_RELAUNCH
+#define TMC_SWEEP_PUBLISH_AT_RELAUNCH 0
 #endif
 
 template <int FAST, bool TILE, bool PROF> struct SweepCtx {
@@ -103,9 +111,8 @@ template <int FAST, bool TILE, bool PROF> struct SweepCtx {
     uint32_t tile_cfg;
     int tile_t;  // tally offset of tile_cfg
 
-    // the step publishes an ended packet (in the kernel's relaunch it measured slower here: the
-    // sweep kernel is held to 64 registers and spilled)
-    static constexpr bool kPublishAtRelaunch = false;
+    // where an ended packet is published (TMC_SWEEP_PUBLISH_AT_RELAUNCH): in the step by default
+    static constexpr bool kPublishAtRelaunch = TMC_SWEEP_PUBLISH_AT_RELAUNCH != 0;
 
     __device__ __forceinline__ void refill(Lane &L) const { ring.refill(L, sched, static_cast<int>(P.threads)); }
     __device__ __forceinline__ uint32_t draw(Lane &L) const { return ring.draw(L); }
@@ -226,10 +233,17 @@ __device__ __forceinline__ void sweep_body(const SweepParams &P) {
     bool items_done = false;
     unsigned ex_mask = 0u;  // warp-uniform: lanes with no photon left to take
     bool alive = false;
+    bool held = false;  // L holds an ended photon whose totals are not yet published
     Lane L;
 
     for (;;) {
         unsigned need = ~__ballot_sync(0xffffffffu, alive) & ~ex_mask;
+        if constexpr (decltype(C)::kPublishAtRelaunch) {
+            if (((need >> lane) & 1u) && held) {  // the lane's last photon ended: publish it
+                finish_photon(L, C);
+                held = false;
+            }
+        }
         while (need) {  // warp-uniform: hand out photons, taking new items as they run out
             const uint32_t avail = it_end - it_next;
             if (avail == 0u) {
@@ -270,6 +284,7 @@ __device__ __forceinline__ void sweep_body(const SweepParams &P) {
                 const int batch = batch_of(id, cf.plan_base, cf.plan_extra, cf.plan_bnd);
                 launch(L, C, id, batch, cf.launch_w);
                 alive = true;
+                held = true;
             }
             need &= ~__ballot_sync(0xffffffffu, mine);
             it_next += take;
